@@ -1,0 +1,37 @@
+"""Load the golden fixtures written by tests/golden/make_golden.py."""
+import os
+
+import numpy as np
+import scipy.sparse as sp
+
+from orbit_b200 import synthetic
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "small_grid.npz")
+_NAMES = ("dP", "Dz", "u", "v", "u_plus", "u_minus", "v_plus", "v_minus", "u_e",
+          "u_plus_e", "u_minus_e", "v_n", "v_plus_n", "v_minus_n", "kxxyy", "kzz",
+          "w_plus", "w_minus", "cmfmc", "kmu", "kmv", "lat", "lon")
+
+
+def load():
+    return dict(np.load(GOLDEN))
+
+
+def met_bin(z, prefix):
+    nz, ny, nx, dlat, dlon, split = z[f"{prefix}meta"]
+    kw = {n: np.array(z[f"{prefix}{n}"]) for n in _NAMES}
+    return synthetic.MetBin(nz=int(nz), ny=int(ny), nx=int(nx), dlat=float(dlat),
+                            dlon=float(dlon), split=bool(split), **kw)
+
+
+def met_list(z):
+    return [met_bin(z, f"met{t}_") for t in range(8)]
+
+
+def species(z):
+    return synthetic.SpeciesFields(vd=z["vd"], wet=z["wet"], loss=z["loss"], emis=z["emis"])
+
+
+def csc(z, prefix):
+    n = len(z[f"{prefix}indptr"]) - 1
+    return sp.csc_matrix((z[f"{prefix}data"], z[f"{prefix}indices"], z[f"{prefix}indptr"]),
+                         shape=(n, n))
