@@ -1,0 +1,181 @@
+/*
+ * liborbit_b200 — C ABI of the B200-native periodic-orbit solver.
+ *
+ * Every entry point returns an int status (ORBIT_OK = 0); on failure
+ * orbit_last_error() returns a message for the calling thread.  Device
+ * buffers are caller-owned (plain device pointers plus sizes); handles
+ * (symbolic analysis, factor batches) own their internal workspace and are
+ * created and destroyed in matching pairs.  Each call takes the CUDA stream
+ * to run on; distinct handles may be used from distinct threads at once.
+ *
+ * Index conventions: cell = k*ny*nx + j*nx + i (reference CellIndexer,
+ * orbit/core/indexing.py:5-45); vectors passed in and out are in this cell
+ * order.  Stencil arrays are [7][N] with directions
+ * {centre, west, east, south, north, below, above}.
+ *
+ * Each declaration cites the reference interface it replaces.
+ */
+#ifndef ORBIT_B200_H_
+#define ORBIT_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* orbit_stream_t; /* == cudaStream_t */
+
+enum {
+  ORBIT_OK = 0,
+  ORBIT_ERR_ARG = 1,       /* bad argument (reference: ValueError) */
+  ORBIT_ERR_NOMEM = 2,     /* device allocation failed */
+  ORBIT_ERR_CUDA = 3,      /* CUDA runtime error */
+  ORBIT_ERR_TIMEOUT = 4,   /* a bounded device spin-wait gave up */
+  ORBIT_ERR_PIVOT = 5,     /* zero or non-finite pivot (reference: umfpack status != 0, solve.py:231) */
+  ORBIT_ERR_NOCONV = 6,    /* GMRES hit maxiter (reference prints a WARNING, orbit.py:184) */
+  ORBIT_ERR_INTERNAL = 7,
+  ORBIT_ERR_NOTFINITE = 8  /* non-finite input or iterate */
+};
+
+enum { ORBIT_PREC_FP64 = 64, ORBIT_PREC_FP32 = 32 };
+
+typedef struct orbit_symbolic_s* orbit_symbolic_t;
+typedef struct orbit_factor_s* orbit_factor_t;
+
+/* Message of the last failed call on this thread. */
+const char* orbit_last_error(void);
+/* Library version string. */
+const char* orbit_version(void);
+
+/* Per-bin averaged meteorology on the device (each pointer nz*ny*nx doubles
+ * unless noted).  Field meaning follows GridData, orbit/core/grid_data.py:19-215. */
+typedef struct {
+  const double* dP;
+  const double* Dz;
+  const double* u;        /* UAvg (west face of each cell) */
+  const double* v;        /* VAvg (south face) */
+  const double* u_plus;   /* UAvg_plus */
+  const double* u_minus;  /* UAvg_minus */
+  const double* v_plus;
+  const double* v_minus;
+  const double* u_e;      /* east outer face, (nz, ny) */
+  const double* u_plus_e; /* (nz, ny) */
+  const double* v_n;      /* north outer face, (nz, nx) */
+  const double* v_plus_n; /* (nz, nx) */
+  const double* kxxyy;
+  const double* kzz;
+  const double* w_plus;   /* interface downward flux, (nz+1, ny, nx) */
+  const double* w_minus;  /* interface upward flux,   (nz+1, ny, nx) */
+  const double* cmfmc;    /* (nz+1, ny, nx) or NULL */
+  const double* kmu;      /* face meander K (non-split mode only) or NULL */
+  const double* kmv;
+  const double* lat;      /* (ny,) degrees */
+  double dlat, dlon;      /* degrees */
+  int split;              /* has_split_fluxes */
+} orbit_met_t;
+
+/* Symbolic analysis of one (nz, ny, nx) domain: geometric nested dissection
+ * into dense supernodes plus the static factor/solve schedules.  Replaces
+ * umfpack_symbolic / compute_metis_ordering (orbit/core/solve.py:88-207,
+ * 299-335); like them it is computed once and reused for every species,
+ * bin and met draw of the domain.  leaf_cells <= 0 selects the default. */
+int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out);
+/* Replaces umfpack_free_symbolic (orbit/core/solve.py:291-296). */
+int orbit_symbolic_destroy(orbit_symbolic_t sym);
+/* info[0..11] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor
+ * elements per instance, front elements per instance, max front, factor
+ * flops, solve items per bin, update-vector length, leaf_cells, max n/m. */
+int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info);
+/* perm[new] = cell (host array of N int32). */
+int orbit_symbolic_perm(orbit_symbolic_t sym, int32_t* perm_host);
+/* Copy a named host array of the analysis (int32 or int64 elements, as the
+ * analysis stores it) for inspection and host-side checks; dst may be NULL to
+ * query *count.  Names: perm, iperm, first, n, m, parent, level, child, uoff,
+ * uidx, rel, ldn, ldm, ldf, fac_off, front_off, level_front_size,
+ * ent_level_off, ent_pos, ent_src, woff, sitems, phase_off, phase_offT,
+ * nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT.  No reference counterpart
+ * (UMFPACK's symbolic object is opaque); it exists so the structure can be
+ * verified on a host without a GPU.  The analysis itself never touches the
+ * device: device copies are made by the first orbit_factor_create. */
+int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int64_t capacity,
+                         int64_t* count);
+
+/* K1: assemble the concentration-form transport block T of one bin as a
+ * 7-point stencil (device, [7][N] doubles), and the per-cell row sum of the
+ * pressure-form block (device, N doubles, may be NULL).  Replaces
+ * assemble_transport_block (orbit/core/operator.py:281-353) with its parts
+ * assemble_horizontal_convdiff (convdiff.py:42-387),
+ * assemble_vertical_advection (advection.py:383-523),
+ * assemble_vertical_diffusion (mixing.py:14-117) and
+ * assemble_cmfmc_transport (convection.py:25-140). */
+int orbit_assemble_transport(int nz, int ny, int nx, const orbit_met_t* met,
+                             double* T_stencil, double* rowsum, orbit_stream_t stream);
+
+/* K7: air-mass-balance row sums |T rho / rho| per day over laterally
+ * interior cells for nbins stencils; writes the interior (nz-1 layers) and
+ * top-layer magnitudes to out_interior / out_top (device, nbins*(nz-1)*(ny-2)*(nx-2)
+ * and nbins*(ny-2)*(nx-2) doubles).  Replaces the row-sum part of
+ * mass_balance_diagnostics (orbit/core/operator.py:598-652). */
+int orbit_mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* T_stencils,
+                            const double* const* rho, double* out_interior, double* out_top,
+                            orbit_stream_t stream);
+
+/* K2: limited horizontal FCT deferred-correction source d_AD for n_vec
+ * concentration vectors on one bin's grid.  c and d are device (n_vec, N).
+ * Replaces compute_horizontal_fct_source (orbit/core/fct.py:459-492). */
+int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
+                     const double* c, double dt, int limited, double* d, orbit_stream_t stream);
+
+/* A batch of n_orbits x 8 numeric factorizations of A = I + dtau (T + diag(sink))
+ * sharing one symbolic.  precision = ORBIT_PREC_FP64 or ORBIT_PREC_FP32.
+ * Replaces _factor_one_bin / _UmfpackLU.__init__ (orbit/core/orbit.py:79-96,
+ * orbit/core/solve.py:210-243). */
+int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit_factor_t* out);
+int orbit_factor_destroy(orbit_factor_t f);
+/* Factor all (or the first n_active) orbits.  T_stencils / sink_diags are host
+ * arrays of n_active*8 device pointers (orbit-major, bin-minor); a sink
+ * pointer may be NULL.  The stencils are copied; callers may free them after
+ * the call returns (stream-ordered). */
+int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_stencils,
+                         const double* const* sink_diags, double dtau, orbit_stream_t stream);
+/* Device bytes held by the factor handle (reference: numeric_bytes, solve.py:233-236). */
+int orbit_factor_bytes(orbit_factor_t f, int64_t* numeric_bytes, int64_t* workspace_bytes);
+
+/* K4: chained solves x <- P_tau x for tau in [tau0, tau1) (trans = 0), or
+ * x <- P_tau^T x for tau = tau1-1 .. tau0 (trans = 1), for n_active orbits, one
+ * persistent launch.  x_in, x_out: device (n_active, N) in cell order.  With
+ * forcing (device (n_active, 8, N), may be NULL) the forward chain solves
+ * P_tau (x + fscale e_tau) and the transposed chain adds fscale e_tau after each
+ * P_tau^T.  Replaces lu.solve(b, trans) chains: apply_monodromy
+ * (orbit.py:99-107), compute_s (orbit.py:110-120), apply_monodromy_adjoint
+ * and compute_s_adjoint (orbit_adjoint.py:36-67).  For FP32 factors,
+ * refine != 0 applies one FP64 iterative-refinement step per bin. */
+int orbit_chain_apply(orbit_factor_t f, int n_active, int trans, int tau0, int tau1,
+                      const double* x_in, double* x_out, const double* forcing, double fscale,
+                      int refine, orbit_stream_t stream);
+
+/* K5: batched periodic-orbit GMRES(restart) solves of (I - M) c0 = s for the
+ * first n_active orbits of a factored batch.  e: device (n_active, 8, N)
+ * emissions; c_warm: device (n_active, N) or NULL; orbit_out: device
+ * (n_active, 9, N); info_out: host (n_active, 8) doubles = {gmres_iters,
+ * residual, periodicity, neg_frac, converged, s_norm, outer_refinements,
+ * matvecs}.  Mixed precision (FP32 factors) runs inner GMRES on the FP32
+ * monodromy inside an FP64 outer refinement of the monodromy residual.
+ * Replaces solve_orbit_one_species (orbit/core/orbit.py:123-210). */
+int orbit_gmres_solve(orbit_factor_t f, int n_active, const double* e, double dtau,
+                      const double* c_warm, double tol, int maxiter, int restart,
+                      double* orbit_out, double* info_out, orbit_stream_t stream);
+
+/* Transposed periodic-orbit solve (I - M^T) lam0 = s_adj with receptors R
+ * (device (n_active, 8, N)); adjoint_out (n_active, 9, N); info_out (n_active, 8)
+ * as above.  Replaces solve_orbit_adjoint_one_species
+ * (orbit/core/orbit_adjoint.py:70-144). */
+int orbit_adjoint_gmres_solve(orbit_factor_t f, int n_active, const double* R,
+                              const double* lam_warm, double tol, int maxiter, int restart,
+                              double* adjoint_out, double* info_out, orbit_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORBIT_B200_H_ */

@@ -1,0 +1,440 @@
+// extern "C" entry points of liborbit_b200 (declared in include/orbit_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "handles.h"
+
+namespace orbit {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int run_factor(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st);
+int launch_chain(orbit_factor_s* f, int B, const int* d_orbit_ids, int trans, int tau0, int tau1,
+                 const double* E, double escale, cudaStream_t st);
+int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau, const double* warm,
+                     double tol, int maxiter, int restart, double* out, double* info, int trans,
+                     cudaStream_t st);
+int chain_apply_impl(orbit_factor_s* f, int n, int trans, int tau0, int tau1, const double* x_in,
+                     double* x_out, const double* forcing, double fscale, int refine, cudaStream_t st);
+int assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T, double* rowsum,
+                       cudaStream_t st);
+int mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* Tst,
+                      const double* const* rho, double* out_int, double* out_top, cudaStream_t st);
+int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
+               int limited, double* d, double* scratch, cudaStream_t st);
+
+namespace {
+
+template <typename T>
+int dalloc(std::vector<void*>& allocs, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("device allocation of ") + std::to_string(count * sizeof(T)) +
+                   " bytes failed: " + cudaGetErrorString(e));
+    return ORBIT_ERR_NOMEM;
+  }
+  allocs.push_back(*p);
+  return ORBIT_OK;
+}
+
+template <typename T>
+int upload(std::vector<void*>& allocs, T** p, const std::vector<T>& v) {
+  int rc = dalloc(allocs, p, v.size());
+  if (rc) return rc;
+  if (!v.empty()) ORBIT_CUDA_TRY(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return ORBIT_OK;
+}
+
+void free_all(std::vector<void*>& allocs) {
+  for (void* p : allocs) cudaFree(p);
+  allocs.clear();
+}
+
+#define ORBIT_TRY(expr)        \
+  do {                         \
+    int _rc = (expr);          \
+    if (_rc != ORBIT_OK) {     \
+      return _rc;              \
+    }                          \
+  } while (0)
+
+int build_device_symbolic(orbit_symbolic_s* h) {
+  const Symbolic& S = h->S;
+  auto& A = h->allocs;
+  DevSym& d = h->d;
+  ORBIT_TRY(upload(A, &d.first, S.first));
+  ORBIT_TRY(upload(A, &d.n, S.n));
+  ORBIT_TRY(upload(A, &d.m, S.m));
+  ORBIT_TRY(upload(A, &d.parent, S.parent));
+  ORBIT_TRY(upload(A, &d.child, S.child));
+  ORBIT_TRY(upload(A, &d.uoff, S.uoff));
+  ORBIT_TRY(upload(A, &d.uidx, S.uidx));
+  ORBIT_TRY(upload(A, &d.rel, S.rel));
+  ORBIT_TRY(upload(A, &d.fac_off, S.fac_off));
+  ORBIT_TRY(upload(A, &d.ldn, S.ldn));
+  ORBIT_TRY(upload(A, &d.ldm, S.ldm));
+  ORBIT_TRY(upload(A, &d.ldf, S.ldf));
+  ORBIT_TRY(upload(A, &d.front_off, S.front_off));
+  ORBIT_TRY(upload(A, &d.woff, S.woff));
+  ORBIT_TRY(upload(A, &d.ent_pos, S.ent_pos));
+  ORBIT_TRY(upload(A, &d.ent_src, S.ent_src));
+  {
+    std::vector<int4> fi(S.fitems.size() / 4);
+    std::memcpy(fi.data(), S.fitems.data(), fi.size() * sizeof(int4));
+    ORBIT_TRY(upload(A, &d.fitems, fi));
+    std::vector<int4> si(S.sitems.size() / 4);
+    std::memcpy(si.data(), S.sitems.data(), si.size() * sizeof(int4));
+    ORBIT_TRY(upload(A, &d.sitems, si));
+  }
+  ORBIT_TRY(upload(A, &d.phase_off, S.phase_off));
+  ORBIT_TRY(upload(A, &d.phase_offT, S.phase_offT));
+  ORBIT_TRY(upload(A, &d.nchunk_fwd, S.nchunk_fwd));
+  ORBIT_TRY(upload(A, &d.nchunk_bwd, S.nchunk_bwd));
+  ORBIT_TRY(upload(A, &d.nchunk_fwdT, S.nchunk_fwdT));
+  ORBIT_TRY(upload(A, &d.nchunk_bwdT, S.nchunk_bwdT));
+  ORBIT_TRY(upload(A, &d.perm, S.perm));
+  ORBIT_TRY(upload(A, &d.iperm, S.iperm));
+  return ORBIT_OK;
+}
+
+constexpr int kDefaultLeaf = 16;
+constexpr int kChunkElems = 8192;
+
+}  // namespace
+}  // namespace orbit
+
+using namespace orbit;
+
+extern "C" {
+
+const char* orbit_last_error(void) { return g_last_error.c_str(); }
+const char* orbit_version(void) { return "orbit_b200 0.1 (sm_100a)"; }
+
+int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out) {
+  if (!out) {
+    set_last_error("out is NULL");
+    return ORBIT_ERR_ARG;
+  }
+  *out = nullptr;
+  orbit_symbolic_s* h = new (std::nothrow) orbit_symbolic_s();
+  if (!h) return ORBIT_ERR_NOMEM;
+  std::string err = build_symbolic(nz, ny, nx, leaf_cells > 0 ? leaf_cells : kDefaultLeaf, kChunkElems, h->S);
+  if (!err.empty()) {
+    set_last_error(err);
+    delete h;
+    return ORBIT_ERR_ARG;
+  }
+  *out = h;
+  return ORBIT_OK;
+}
+
+int orbit_symbolic_destroy(orbit_symbolic_t sym) {
+  if (!sym) return ORBIT_OK;
+  free_all(sym->allocs);
+  delete sym;
+  return ORBIT_OK;
+}
+
+int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info) {
+  if (!sym || !info) {
+    set_last_error("null argument");
+    return ORBIT_ERR_ARG;
+  }
+  const Symbolic& S = sym->S;
+  int64_t v[12] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
+                   (int64_t)S.factor_flops, S.items_per_bin, S.w_size, S.leaf_cells, S.max_nm};
+  for (int i = 0; i < n_info && i < 12; ++i) info[i] = v[i];
+  return ORBIT_OK;
+}
+
+int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int64_t capacity,
+                         int64_t* count) {
+  if (!sym || !name) {
+    set_last_error("null argument");
+    return ORBIT_ERR_ARG;
+  }
+  const Symbolic& S = sym->S;
+  const void* src = nullptr;
+  int64_t cnt = 0;
+  size_t es = 4;
+  std::string nm(name);
+#define ORBIT_ARR(key, vec)                  \
+  if (nm == key) {                           \
+    src = S.vec.data();                      \
+    cnt = (int64_t)S.vec.size();             \
+    es = sizeof(S.vec[0]);                   \
+  }
+  ORBIT_ARR("perm", perm) ORBIT_ARR("iperm", iperm) ORBIT_ARR("first", first) ORBIT_ARR("n", n)
+  ORBIT_ARR("m", m) ORBIT_ARR("parent", parent) ORBIT_ARR("level", level) ORBIT_ARR("child", child)
+  ORBIT_ARR("uoff", uoff) ORBIT_ARR("uidx", uidx) ORBIT_ARR("rel", rel) ORBIT_ARR("ldn", ldn)
+  ORBIT_ARR("ldm", ldm) ORBIT_ARR("ldf", ldf) ORBIT_ARR("fac_off", fac_off)
+  ORBIT_ARR("front_off", front_off) ORBIT_ARR("level_front_size", level_front_size)
+  ORBIT_ARR("ent_level_off", ent_level_off) ORBIT_ARR("ent_pos", ent_pos) ORBIT_ARR("ent_src", ent_src)
+  ORBIT_ARR("woff", woff) ORBIT_ARR("sitems", sitems) ORBIT_ARR("phase_off", phase_off)
+  ORBIT_ARR("phase_offT", phase_offT) ORBIT_ARR("nchunk_fwd", nchunk_fwd)
+  ORBIT_ARR("nchunk_bwd", nchunk_bwd) ORBIT_ARR("nchunk_fwdT", nchunk_fwdT)
+  ORBIT_ARR("nchunk_bwdT", nchunk_bwdT)
+#undef ORBIT_ARR
+  if (!src && cnt == 0 && nm != "sitems") {
+    bool known = false;
+    for (const char* k : {"perm", "iperm", "first", "n", "m", "parent", "level", "child", "uoff", "uidx",
+                          "rel", "ldn", "ldm", "ldf", "fac_off", "front_off", "level_front_size",
+                          "ent_level_off", "ent_pos", "ent_src", "woff", "phase_off", "phase_offT",
+                          "nchunk_fwd", "nchunk_bwd", "nchunk_fwdT", "nchunk_bwdT"})
+      known = known || nm == k;
+    if (!known) {
+      set_last_error("unknown symbolic array " + nm);
+      return ORBIT_ERR_ARG;
+    }
+  }
+  if (count) *count = cnt;
+  if (dst) {
+    if (capacity < cnt) {
+      set_last_error("destination too small");
+      return ORBIT_ERR_ARG;
+    }
+    if (cnt) std::memcpy(dst, src, (size_t)cnt * es);
+  }
+  return ORBIT_OK;
+}
+
+int orbit_symbolic_perm(orbit_symbolic_t sym, int32_t* perm_host) {
+  if (!sym || !perm_host) {
+    set_last_error("null argument");
+    return ORBIT_ERR_ARG;
+  }
+  std::memcpy(perm_host, sym->S.perm.data(), sym->S.perm.size() * sizeof(int32_t));
+  return ORBIT_OK;
+}
+
+int orbit_assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T_stencil,
+                             double* rowsum, orbit_stream_t stream) {
+  if (!met || !T_stencil || nz < 1 || ny < 2 || nx < 2) {
+    set_last_error("orbit_assemble_transport: bad arguments (need nz>=1, ny>=2, nx>=2)");
+    return ORBIT_ERR_ARG;
+  }
+  if (!met->dP || !met->Dz || !met->u || !met->v || !met->kxxyy || !met->kzz || !met->w_plus ||
+      !met->w_minus || !met->lat || (met->split && (!met->u_plus || !met->u_minus || !met->v_plus ||
+                                                    !met->v_minus || !met->u_plus_e || !met->v_plus_n)) ||
+      (!met->split && (!met->u_e || !met->v_n))) {
+    set_last_error("orbit_assemble_transport: missing meteorology field");
+    return ORBIT_ERR_ARG;
+  }
+  return assemble_transport(nz, ny, nx, met, T_stencil, rowsum, (cudaStream_t)stream);
+}
+
+int orbit_mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* T_stencils,
+                            const double* const* rho, double* out_interior, double* out_top,
+                            orbit_stream_t stream) {
+  if (nbins < 1 || ny < 3 || nx < 3 || !T_stencils || !rho || !out_interior || !out_top) {
+    set_last_error("orbit_mass_balance_rows: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const double** d = nullptr;
+  ORBIT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(double*) * 2 * nbins, st));
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(d, T_stencils, sizeof(double*) * nbins, cudaMemcpyHostToDevice, st));
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(d + nbins, rho, sizeof(double*) * nbins, cudaMemcpyHostToDevice, st));
+  int rc = mass_balance_rows(nz, ny, nx, nbins, d, d + nbins, out_interior, out_top, st);
+  cudaFreeAsync(d, st);
+  ORBIT_CUDA_TRY(cudaStreamSynchronize(st));
+  return rc;
+}
+
+int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
+                     int limited, double* d, orbit_stream_t stream) {
+  if (!met || !c || !d || n_vec < 1 || nz < 1 || ny < 1 || nx < 1 || !(dt > 0)) {
+    set_last_error("orbit_fct_source: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t N = (int64_t)nz * ny * nx;
+  double* scratch = nullptr;
+  ORBIT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(double) * 3 * N * n_vec, st));
+  int rc = fct_source(nz, ny, nx, met, n_vec, c, dt, limited, d, scratch, st);
+  cudaFreeAsync(scratch, st);
+  return rc;
+}
+
+int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit_factor_t* out) {
+  if (!sym || !out || n_orbits < 1 || (precision != ORBIT_PREC_FP64 && precision != ORBIT_PREC_FP32)) {
+    set_last_error("orbit_factor_create: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  *out = nullptr;
+  {
+    // device copies of the symbolic arrays are made on first use
+    std::lock_guard<std::mutex> lk(sym->mu);
+    if (!sym->uploaded) {
+      int rc0 = build_device_symbolic(sym);
+      if (rc0) {
+        free_all(sym->allocs);
+        sym->d = DevSym();
+        return rc0;
+      }
+      cudaGetDevice(&sym->device);
+      sym->uploaded = true;
+    }
+  }
+  orbit_factor_s* f = new (std::nothrow) orbit_factor_s();
+  if (!f) return ORBIT_ERR_NOMEM;
+  f->sym = sym;
+  f->n_orbits = n_orbits;
+  f->precision = precision;
+  cudaGetDevice(&f->device);
+  const Symbolic& S = sym->S;
+  const int64_t N = S.N;
+  const size_t vb = precision == ORBIT_PREC_FP32 ? 4 : 8;
+  const int64_t n_inst = (int64_t)n_orbits * 8;
+  auto& A = f->allocs;
+  int rc = ORBIT_OK;
+  auto fail = [&](int code) {
+    free_all(A);
+    delete f;
+    return code;
+  };
+  // fronts: group size from a budget
+  const size_t budget = (size_t)8 << 30;
+  int64_t per_inst = 2 * S.front_buf_size * (int64_t)vb;
+  int64_t G = per_inst > 0 ? (int64_t)(budget / per_inst) : n_inst;
+  G = std::max<int64_t>(1, std::min<int64_t>(G, n_inst));
+  f->front_group = (int)G;
+  if ((rc = dalloc(A, reinterpret_cast<unsigned char**>(&f->factors), (size_t)n_inst * S.fac_size * vb))) return fail(rc);
+  if ((rc = dalloc(A, reinterpret_cast<unsigned char**>(&f->fronts), (size_t)2 * G * S.front_buf_size * vb))) return fail(rc);
+  if ((rc = dalloc(A, &f->A_stencil, (size_t)n_inst * 7 * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->d_Tptr, (size_t)n_inst))) return fail(rc);
+  if ((rc = dalloc(A, &f->d_Dptr, (size_t)n_inst))) return fail(rc);
+  if ((rc = dalloc(A, &f->X, (size_t)n_orbits * 9 * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->Ybuf, (size_t)n_orbits * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->Wbuf, (size_t)n_orbits * S.w_size))) return fail(rc);
+  if ((rc = dalloc(A, &f->counters, (size_t)n_orbits * 16 * S.nsuper))) return fail(rc);
+  if ((rc = dalloc(A, &f->E, (size_t)n_orbits * 8 * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->tmpv, (size_t)n_orbits * 15 * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->orbit_ids, (size_t)n_orbits))) return fail(rc);
+  if ((rc = dalloc(A, &f->task_counter, (size_t)1 + n_orbits))) return fail(rc);
+  if ((rc = dalloc(A, &f->status, (size_t)1))) return fail(rc);
+  f->restart_cap = 31;
+  if ((rc = dalloc(A, &f->V, (size_t)n_orbits * 33 * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->Hd, (size_t)n_orbits * 33 * 32))) return fail(rc);
+  if ((rc = dalloc(A, &f->gv, (size_t)n_orbits * 33))) return fail(rc);
+  if ((rc = dalloc(A, &f->cs, (size_t)n_orbits * 32))) return fail(rc);
+  if ((rc = dalloc(A, &f->sn, (size_t)n_orbits * 32))) return fail(rc);
+  if ((rc = dalloc(A, &f->red, (size_t)n_orbits * 33 + (size_t)n_orbits * 32 * 33 * 48))) return fail(rc);
+  if ((rc = dalloc(A, &f->scal, (size_t)n_orbits * 16))) return fail(rc);
+  if (cudaMallocHost(reinterpret_cast<void**>(&f->h_status), sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&f->h_scal), sizeof(double) * 16 * n_orbits) != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error("pinned host allocation failed");
+    return fail(ORBIT_ERR_NOMEM);
+  }
+  if (cudaMemset(f->status, 0, sizeof(int)) != cudaSuccess) return fail(ORBIT_ERR_CUDA);
+  *out = f;
+  return ORBIT_OK;
+}
+
+int orbit_factor_destroy(orbit_factor_t f) {
+  if (!f) return ORBIT_OK;
+  cudaDeviceSynchronize();
+  free_all(f->allocs);
+  if (f->h_status) cudaFreeHost(f->h_status);
+  if (f->h_scal) cudaFreeHost(f->h_scal);
+  delete f;
+  return ORBIT_OK;
+}
+
+int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_stencils,
+                         const double* const* sink_diags, double dtau, orbit_stream_t stream) {
+  if (!f || !T_stencils || n_active < 1 || n_active > f->n_orbits || !(dtau > 0)) {
+    set_last_error("orbit_factor_numeric: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  for (int i = 0; i < n_active * 8; ++i)
+    if (!T_stencils[i]) {
+      set_last_error("orbit_factor_numeric: NULL transport stencil");
+      return ORBIT_ERR_ARG;
+    }
+  std::lock_guard<std::mutex> lk(f->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<const double*> dp(n_active * 8, nullptr);
+  if (sink_diags)
+    for (int i = 0; i < n_active * 8; ++i) dp[i] = sink_diags[i];
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Tptr, T_stencils, sizeof(double*) * n_active * 8, cudaMemcpyHostToDevice, st));
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Dptr, dp.data(), sizeof(double*) * n_active * 8, cudaMemcpyHostToDevice, st));
+  ORBIT_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(int), st));
+  int rc = run_factor(f, n_active, dtau, st);
+  if (rc) return rc;
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->h_status, f->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ORBIT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (*f->h_status != 0) {
+    set_last_error("zero or non-finite pivot in the numeric factorization");
+    return *f->h_status;
+  }
+  f->n_factored = n_active;
+  f->dtau = dtau;
+  return ORBIT_OK;
+}
+
+int orbit_factor_bytes(orbit_factor_t f, int64_t* numeric_bytes, int64_t* workspace_bytes) {
+  if (!f) {
+    set_last_error("null handle");
+    return ORBIT_ERR_ARG;
+  }
+  const Symbolic& S = f->sym->S;
+  const int64_t vb = f->precision == ORBIT_PREC_FP32 ? 4 : 8;
+  if (numeric_bytes) *numeric_bytes = (int64_t)f->n_orbits * 8 * S.fac_size * vb;
+  if (workspace_bytes)
+    *workspace_bytes = (int64_t)2 * f->front_group * S.front_buf_size * vb +
+                       (int64_t)f->n_orbits * (7 * 8 + 9 + 1 + 8 + 15 + 33) * S.N * 8;
+  return ORBIT_OK;
+}
+
+int orbit_chain_apply(orbit_factor_t f, int n_active, int trans, int tau0, int tau1, const double* x_in,
+                      double* x_out, const double* forcing, double fscale, int refine,
+                      orbit_stream_t stream) {
+  if (!f || !x_in || !x_out || n_active < 1 || n_active > f->n_factored || tau0 < 0 || tau1 > 8 ||
+      tau0 >= tau1) {
+    set_last_error("orbit_chain_apply: bad arguments (factor first; 0 <= tau0 < tau1 <= 8)");
+    return ORBIT_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(f->mu);
+  return chain_apply_impl(f, n_active, trans, tau0, tau1, x_in, x_out, forcing, fscale, refine,
+                          (cudaStream_t)stream);
+}
+
+int orbit_gmres_solve(orbit_factor_t f, int n_active, const double* e, double dtau, const double* c_warm,
+                      double tol, int maxiter, int restart, double* orbit_out, double* info_out,
+                      orbit_stream_t stream) {
+  if (!f || !e || !orbit_out || !info_out || n_active < 1 || n_active > f->n_factored || !(tol > 0) ||
+      maxiter < 1) {
+    set_last_error("orbit_gmres_solve: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(f->mu);
+  return orbit_solve_impl(f, n_active, e, dtau, c_warm, tol, maxiter, restart, orbit_out, info_out, 0,
+                          (cudaStream_t)stream);
+}
+
+int orbit_adjoint_gmres_solve(orbit_factor_t f, int n_active, const double* R, const double* lam_warm,
+                              double tol, int maxiter, int restart, double* adjoint_out, double* info_out,
+                              orbit_stream_t stream) {
+  if (!f || !R || !adjoint_out || !info_out || n_active < 1 || n_active > f->n_factored || !(tol > 0) ||
+      maxiter < 1) {
+    set_last_error("orbit_adjoint_gmres_solve: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(f->mu);
+  return orbit_solve_impl(f, n_active, R, 1.0, lam_warm, tol, maxiter, restart, adjoint_out, info_out, 1,
+                          (cudaStream_t)stream);
+}
+
+}  // extern "C"

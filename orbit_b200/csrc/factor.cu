@@ -1,0 +1,511 @@
+// K3: batched numeric factorization of A = I + dtau (T + diag(sink)) on the
+// dense supernodes of the symbolic analysis.
+//
+// Replaces the reference's per-bin sparse LU (_factor_one_bin ->
+// umfpack_di_numeric / scipy splu; orbit/core/orbit.py:79-96,
+// orbit/core/solve.py:210-243).  A is strictly row-diagonally dominant
+// (I plus an M-matrix times dtau), so no pivoting is needed; the reference's
+// SuperLU runs also pivot on the diagonal (perm_r == perm_c).
+//
+// Each supernode front F = [F11 F12; F21 F22] (own rows first, then the
+// ancestor rows of its update set) is assembled from the stencil and the
+// children's Schur complements (extend-add), partially factored by a blocked
+// right-looking LU, and stored for the solve as
+//   SQ = strict_lower(inv(L11)) + upper(inv(U11))   (n x n)
+//   Pb = -L21 inv(L11)                              (m x n)
+//   Qr = -inv(U11) U12                              (n x m)
+// so that every supernode step of the triangular solves is a dense
+// matrix-vector product with no intra-supernode dependency.  The Schur
+// complement F22 - L21 U12 stays in the front for the parent.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "common.cuh"
+#include "handles.h"
+
+namespace orbit {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kLdS = 65;
+
+template <typename T>
+struct Ld {
+  const T* p;
+  int ld, rows, cols, mask, tri;
+  __device__ __forceinline__ T operator()(int r, int c) const {
+    if (r >= rows || c >= cols) return T(0);
+    if (mask == 1) {
+      int d = c - r;
+      if (d > tri) return T(0);
+      if (d == tri) return T(1);
+    } else if (mask == 2) {
+      if (c - r < tri) return T(0);
+    }
+    return p[(int64_t)r * ld + c];
+  }
+};
+
+template <typename T>
+struct LdS {  // operand held in shared memory (ld kLdS)
+  const T* p;
+  int rows, cols;
+  __device__ __forceinline__ T operator()(int r, int c) const {
+    if (r >= rows || c >= cols) return T(0);
+    return p[r * kLdS + c];
+  }
+};
+
+template <typename T, class LA, class LB>
+__device__ __forceinline__ void mma_tile(T (&acc)[4][4], int K, const LA& la, const LB& lb, T* As,
+                                         T* Bs) {
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int k0 = 0; k0 < K; k0 += 16) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int e = tid + q * kThreads;
+      int r = e >> 4, kk = e & 15;
+      As[kk * kLdS + r] = la(r, k0 + kk);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int e = tid + q * kThreads;
+      int kk = e >> 6, c = e & 63;
+      Bs[kk * kLdS + c] = lb(k0 + kk, c);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk * kLdS + ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk * kLdS + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void zero_acc(T (&acc)[4][4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+}
+
+struct FactorDev {
+  const int32_t *n, *m, *parent, *rel, *ldn, *ldm, *ldf;
+  const int64_t *uoff, *fac_off, *front_off;
+  const int4* items;
+  int64_t fac_size, front_buf;
+  int group;  // instances per front group
+};
+
+template <typename T>
+__global__ void k_zero(T* fronts, int64_t count, int64_t stride) {
+  T* f = fronts + (int64_t)blockIdx.y * stride;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < count;
+       e += (int64_t)gridDim.x * blockDim.x)
+    f[e] = T(0);
+}
+
+template <typename T>
+__global__ void k_scatter(T* fronts, int64_t stride, const int64_t* ent_pos, const int32_t* ent_src,
+                          int64_t e0, int64_t ne, const double* const* Tp, const double* const* Dp,
+                          int inst_base, int64_t N, double dtau) {
+  const int inst = inst_base + blockIdx.y;
+  const double* Tv = Tp[inst];
+  const double* Dv = Dp[inst];
+  T* f = fronts + (int64_t)blockIdx.y * stride;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int32_t src = ent_src[e0 + e];
+    int d = (int)(src / N);
+    int64_t cell = src - (int64_t)d * N;
+    double t = Tv[src];
+    double val = d == 0 ? 1.0 + dtau * (t + (Dv ? Dv[cell] : 0.0)) : dtau * t;
+    f[ent_pos[e0 + e]] = (T)val;
+  }
+}
+
+// FP64 copy of the assembled stencil of A for iterative refinement.
+__global__ void k_copy_A(double* A, const double* const* Tp, const double* const* Dp,
+                         int inst_base, int64_t N, double dtau) {
+  const int inst = inst_base + blockIdx.y;
+  const double* Tv = Tp[inst];
+  const double* Dv = Dp[inst];
+  double* out = A + (int64_t)inst * 7 * N;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 7 * N;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    double t = Tv[e];
+    out[e] = e < N ? 1.0 + dtau * (t + (Dv ? Dv[e] : 0.0)) : dtau * t;
+  }
+}
+
+template <typename T>
+__global__ void k_extend(FactorDev D, T* fr_par, const T* fr_child, int64_t i0) {
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int c = it.x, rb = it.y;
+  const int p = D.parent[c];
+  const int nc = D.n[c], mc = D.m[c];
+  const int ldc = D.ldf[c], ldp = D.ldf[p];
+  const T* S = fr_child + (int64_t)blockIdx.y * D.front_buf + D.front_off[c] + (int64_t)nc * ldc + nc;
+  T* F = fr_par + (int64_t)blockIdx.y * D.front_buf + D.front_off[p];
+  const int32_t* rel = D.rel + D.uoff[c];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = rb * 32 + warp; i < min(rb * 32 + 32, mc); i += kThreads / 32) {
+    const int64_t prow = (int64_t)rel[i] * ldp;
+    for (int j = lane; j < mc; j += 32) F[prow + rel[j]] += S[(int64_t)i * ldc + j];
+  }
+}
+
+template <typename T>
+__global__ void k_diag(FactorDev D, T* fronts, T* factors, int64_t i0, int p0, int inst_base,
+                       int* status) {
+  extern __shared__ unsigned char smem_raw[];
+  T* Dm = reinterpret_cast<T*>(smem_raw);
+  T* Li = Dm + 64 * kLdS;
+  T* Ui = Li + 64 * kLdS;
+  const int s = D.items[i0 + blockIdx.x].x;
+  const int n = D.n[s];
+  const int nb = min(64, n - p0);
+  const int ldf = D.ldf[s], ldn = D.ldn[s];
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < nb * nb; e += kThreads) {
+    int r = e / nb, c = e % nb;
+    Dm[r * kLdS + c] = F[(int64_t)(p0 + r) * ldf + p0 + c];
+  }
+  __syncthreads();
+  for (int k = 0; k < nb; ++k) {
+    T piv = Dm[k * kLdS + k];
+    if (tid == 0 && (!(piv == piv) || piv == T(0) || isinf((double)piv)))
+      raise_status(status, ORBIT_ERR_PIVOT);
+    for (int i = k + 1 + tid; i < nb; i += kThreads) Dm[i * kLdS + k] /= piv;
+    __syncthreads();
+    const int w = nb - k - 1;
+    for (int e = tid; e < w * w; e += kThreads) {
+      int i = k + 1 + e / w, j = k + 1 + e % w;
+      Dm[i * kLdS + j] -= Dm[i * kLdS + k] * Dm[k * kLdS + j];
+    }
+    __syncthreads();
+  }
+  if (tid < 64) {
+    const int j = tid;
+    if (j < nb) {
+      for (int i = 0; i < j; ++i) Li[i * kLdS + j] = T(0);
+      Li[j * kLdS + j] = T(1);
+      for (int i = j + 1; i < nb; ++i) {
+        T acc = T(0);
+        for (int k = j; k < i; ++k) acc -= Dm[i * kLdS + k] * Li[k * kLdS + j];
+        Li[i * kLdS + j] = acc;
+      }
+    }
+  } else if (tid < 128) {
+    const int j = tid - 64;
+    if (j < nb) {
+      for (int i = j + 1; i < nb; ++i) Ui[i * kLdS + j] = T(0);
+      Ui[j * kLdS + j] = T(1) / Dm[j * kLdS + j];
+      for (int i = j - 1; i >= 0; --i) {
+        T acc = T(0);
+        for (int k = i + 1; k <= j; ++k) acc += Dm[i * kLdS + k] * Ui[k * kLdS + j];
+        Ui[i * kLdS + j] = -acc / Dm[i * kLdS + i];
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < nb * nb; e += kThreads) {
+    int r = e / nb, c = e % nb;
+    F[(int64_t)(p0 + r) * ldf + p0 + c] = Dm[r * kLdS + c];
+    SQ[(int64_t)(p0 + r) * ldn + p0 + c] = r > c ? Li[r * kLdS + c] : Ui[r * kLdS + c];
+  }
+}
+
+template <typename T>
+__global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, int p0,
+                        int inst_base) {
+  extern __shared__ unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + 16 * kLdS;
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, kind = it.y, ch = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s];
+  const int nb = min(64, n - p0);
+  const int q0 = p0 + nb;
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  const T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  T acc[4][4];
+  zero_acc(acc);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  if (kind == 0) {
+    const int c0 = q0 + 64 * ch, w = min(64, n + m - c0);
+    Ld<T> A{SQ + (int64_t)p0 * ldn + p0, ldn, nb, nb, 1, 0};
+    Ld<T> B{F + (int64_t)p0 * ldf + c0, ldf, nb, w, 0, 0};
+    mma_tile(acc, nb, A, B, As, Bs);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int r = ty + 16 * i, c = tx + 16 * j;
+        if (r < nb && c < w) F[(int64_t)(p0 + r) * ldf + c0 + c] = acc[i][j];
+      }
+  } else {
+    const int r0 = q0 + 64 * ch, h = min(64, n + m - r0);
+    Ld<T> A{F + (int64_t)r0 * ldf + p0, ldf, h, nb, 0, 0};
+    Ld<T> B{SQ + (int64_t)p0 * ldn + p0, ldn, nb, nb, 2, 0};
+    mma_tile(acc, nb, A, B, As, Bs);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int r = ty + 16 * i, c = tx + 16 * j;
+        if (r < h && c < nb) F[(int64_t)(r0 + r) * ldf + p0 + c] = acc[i][j];
+      }
+  }
+}
+
+template <typename T>
+__global__ void k_update(FactorDev D, T* fronts, int64_t i0, int p0) {
+  extern __shared__ unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + 16 * kLdS;
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, tr = it.y, tc = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
+  const int nb = min(64, n - p0);
+  const int q0 = p0 + nb;
+  const int r0 = q0 + 64 * tr, c0 = q0 + 64 * tc;
+  const int h = min(64, n + m - r0), w = min(64, n + m - c0);
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  T acc[4][4];
+  zero_acc(acc);
+  Ld<T> A{F + (int64_t)r0 * ldf + p0, ldf, h, nb, 0, 0};
+  Ld<T> B{F + (int64_t)p0 * ldf + c0, ldf, nb, w, 0, 0};
+  mma_tile(acc, nb, A, B, As, Bs);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int r = ty + 16 * i, c = tx + 16 * j;
+      if (r < h && c < w) F[(int64_t)(r0 + r) * ldf + c0 + c] -= acc[i][j];
+    }
+}
+
+template <typename T>
+__global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int inst_base) {
+  extern __shared__ unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + 16 * kLdS;
+  T* Xs = Bs + 16 * kLdS;
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, kind = it.y, jb = it.z, t = it.w;
+  const int n = D.n[s], ldf = D.ldf[s], ldn = D.ldn[s];
+  const T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[4][4];
+  zero_acc(acc);
+  if (kind == 0) {
+    // Linv block (t, jb): -Linv_tt * sum_{k=jb}^{t-1} L_tk Linv_k,jb
+    const int r0 = 64 * t, h = min(64, n - r0), c0 = 64 * jb;
+    for (int k = jb; k < t; ++k) {
+      Ld<T> A{F + (int64_t)r0 * ldf + 64 * k, ldf, h, 64, 0, 0};
+      Ld<T> B{SQ + (int64_t)(64 * k) * ldn + c0, ldn, 64, 64, k == jb ? 1 : 0, 0};
+      mma_tile(acc, 64, A, B, As, Bs);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) Xs[(ty + 16 * i) * kLdS + tx + 16 * j] = acc[i][j];
+    __syncthreads();
+    zero_acc(acc);
+    Ld<T> A{SQ + (int64_t)r0 * ldn + r0, ldn, h, h, 1, 0};
+    LdS<T> B{Xs, h, 64};
+    mma_tile(acc, h, A, B, As, Bs);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int r = ty + 16 * i, c = tx + 16 * j;
+        if (r < h) SQ[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
+      }
+  } else {
+    // Uinv block (jb, t): -(sum_{k=jb}^{t-1} Uinv_jb,k U_kt) Uinv_tt
+    const int r0 = 64 * jb, c0 = 64 * t, w = min(64, n - c0);
+    for (int k = jb; k < t; ++k) {
+      Ld<T> A{SQ + (int64_t)r0 * ldn + 64 * k, ldn, 64, 64, k == jb ? 2 : 0, 0};
+      Ld<T> B{F + (int64_t)(64 * k) * ldf + c0, ldf, 64, w, 0, 0};
+      mma_tile(acc, 64, A, B, As, Bs);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) Xs[(ty + 16 * i) * kLdS + tx + 16 * j] = acc[i][j];
+    __syncthreads();
+    zero_acc(acc);
+    LdS<T> A{Xs, 64, w};
+    Ld<T> B{SQ + (int64_t)c0 * ldn + c0, ldn, w, w, 2, 0};
+    mma_tile(acc, w, A, B, As, Bs);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int r = ty + 16 * i, c = tx + 16 * j;
+        if (c < w) SQ[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
+      }
+  }
+}
+
+template <typename T>
+__global__ void k_prod(FactorDev D, const T* fronts, T* factors, int64_t i0, int inst_base) {
+  extern __shared__ unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + 16 * kLdS;
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, kind = it.y, a = it.z, b = it.w;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s], ldm = D.ldm[s];
+  const T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  const int nbk = (n + 63) / 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[4][4];
+  zero_acc(acc);
+  if (kind == 0) {
+    const int r0 = 64 * a, h = min(64, m - r0), c0 = 64 * b, w = min(64, n - c0);
+    for (int kb = b; kb < nbk; ++kb) {
+      const int kw = min(64, n - 64 * kb);
+      Ld<T> A{F + (int64_t)(n + r0) * ldf + 64 * kb, ldf, h, kw, 0, 0};
+      Ld<T> B{SQ + (int64_t)(64 * kb) * ldn + c0, ldn, kw, w, kb == b ? 1 : 0, 0};
+      mma_tile(acc, kw, A, B, As, Bs);
+    }
+    T* Pb = SQ + (int64_t)n * ldn;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int r = ty + 16 * i, c = tx + 16 * j;
+        if (r < h && c < w) Pb[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
+      }
+  } else {
+    const int r0 = 64 * a, h = min(64, n - r0), c0 = 64 * b, w = min(64, m - c0);
+    for (int kb = a; kb < nbk; ++kb) {
+      const int kw = min(64, n - 64 * kb);
+      Ld<T> A{SQ + (int64_t)r0 * ldn + 64 * kb, ldn, h, kw, kb == a ? 2 : 0, 0};
+      Ld<T> B{F + (int64_t)(64 * kb) * ldf + n + c0, ldf, kw, w, 0, 0};
+      mma_tile(acc, kw, A, B, As, Bs);
+    }
+    T* Qr = SQ + (int64_t)(n + m) * ldn;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int r = ty + 16 * i, c = tx + 16 * j;
+        if (r < h && c < w) Qr[(int64_t)(r0 + r) * ldm + c0 + c] = -acc[i][j];
+      }
+  }
+}
+
+inline int clamp_grid(int64_t blocks) {
+  if (blocks < 1) return 1;
+  if (blocks > (1 << 20)) return 1 << 20;
+  return (int)blocks;
+}
+
+template <typename T>
+int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) {
+  orbit_symbolic_s* sy = f->sym;
+  const Symbolic& S = sy->S;
+  FactorDev D;
+  D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent; D.rel = sy->d.rel;
+  D.ldn = sy->d.ldn; D.ldm = sy->d.ldm; D.ldf = sy->d.ldf;
+  D.uoff = sy->d.uoff; D.fac_off = sy->d.fac_off; D.front_off = sy->d.front_off;
+  D.items = sy->d.fitems;
+  D.fac_size = S.fac_size;
+  D.front_buf = S.front_buf_size;
+  D.group = f->front_group;
+  T* factors = reinterpret_cast<T*>(f->factors);
+  T* fronts = reinterpret_cast<T*>(f->fronts);
+  const int n_inst = n_active * 8;
+  const size_t sm_gemm = 2 * 16 * kLdS * sizeof(T);
+  const size_t sm_inv = sm_gemm + 64 * kLdS * sizeof(T);
+  const size_t sm_diag = 3 * 64 * kLdS * sizeof(T);
+  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_diag));
+  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_inv));
+  {
+    dim3 g(clamp_grid((7 * S.N + 255) / 256), n_inst);
+    k_copy_A<<<g, 256, 0, st>>>(f->A_stencil, f->d_Tptr, f->d_Dptr, 0, S.N, dtau);
+    ORBIT_CUDA_TRY(cudaGetLastError());
+  }
+  for (int base = 0; base < n_inst; base += f->front_group) {
+    const int G = std::min(f->front_group, n_inst - base);
+    for (const FactorLaunch& L : S.fsched) {
+      T* cur = fronts + (int64_t)(L.level & 1) * f->front_group * S.front_buf_size;
+      T* chl = fronts + (int64_t)((L.level + 1) & 1) * f->front_group * S.front_buf_size;
+      if (L.items <= 0) continue;
+      switch (L.kind) {
+        case FactorLaunch::ZERO: {
+          dim3 g(clamp_grid((L.items + 255) / 256), G);
+          k_zero<T><<<g, 256, 0, st>>>(cur, L.items, S.front_buf_size);
+          break;
+        }
+        case FactorLaunch::SCATTER: {
+          dim3 g(clamp_grid((L.items + 255) / 256), G);
+          k_scatter<T><<<g, 256, 0, st>>>(cur, S.front_buf_size, sy->d.ent_pos, sy->d.ent_src,
+                                          L.item_off, L.items, f->d_Tptr, f->d_Dptr, base, S.N, dtau);
+          break;
+        }
+        case FactorLaunch::EXTEND: {
+          dim3 g((unsigned)L.items, G);
+          k_extend<T><<<g, kThreads, 0, st>>>(D, cur, chl, L.item_off);
+          break;
+        }
+        case FactorLaunch::DIAG: {
+          dim3 g((unsigned)L.items, G);
+          k_diag<T><<<g, kThreads, sm_diag, st>>>(D, cur, factors, L.item_off, L.p0, base, f->status);
+          break;
+        }
+        case FactorLaunch::PANEL: {
+          dim3 g((unsigned)L.items, G);
+          k_panel<T><<<g, kThreads, sm_gemm, st>>>(D, cur, factors, L.item_off, L.p0, base);
+          break;
+        }
+        case FactorLaunch::UPDATE: {
+          dim3 g((unsigned)L.items, G);
+          k_update<T><<<g, kThreads, sm_gemm, st>>>(D, cur, L.item_off, L.p0);
+          break;
+        }
+        case FactorLaunch::INV: {
+          dim3 g((unsigned)L.items, G);
+          k_inv<T><<<g, kThreads, sm_inv, st>>>(D, cur, factors, L.item_off, base);
+          break;
+        }
+        case FactorLaunch::PROD: {
+          dim3 g((unsigned)L.items, G);
+          k_prod<T><<<g, kThreads, sm_gemm, st>>>(D, cur, factors, L.item_off, base);
+          break;
+        }
+      }
+      ORBIT_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  return ORBIT_OK;
+}
+
+}  // namespace
+
+int run_factor(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) {
+  if (f->precision == ORBIT_PREC_FP32) return run_factor_t<float>(f, n_active, dtau, st);
+  return run_factor_t<double>(f, n_active, dtau, st);
+}
+
+}  // namespace orbit

@@ -1,0 +1,221 @@
+// K2: Zalesak-limited horizontal FCT deferred-correction source.
+//
+// Replaces compute_horizontal_fct_source (orbit/core/fct.py:459-492) with its
+// helpers _vanleer_phi (fct.py:235-247), _horizontal_antidiffusive
+// (fct.py:256-357, no ghost cells), _zalesak_2d (fct.py:381-447) and
+// _net_antidiffusive_into_cells (fct.py:360-378).  Pass 1 computes, per cell,
+// the Zalesak ratios R+/R- from the four face fluxes touching it and the
+// 5-point bounds; pass 2 limits every face with the ratios of its two cells
+// and forms d = -div(C A) times rho.  Face fluxes are recomputed where needed
+// rather than stored (each needs at most four cells along its axis).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace orbit {
+
+namespace {
+
+constexpr double kEarthRadius = 6378137.0;
+constexpr double kGravity = 9.80665;
+constexpr double kDegToRad = 3.14159265358979323846 / 180.0;
+
+struct FctGeom {
+  orbit_met_t g;
+  int nz, ny, nx;
+  double dt;
+};
+
+__device__ __forceinline__ double rho_at(const orbit_met_t& g, int64_t c) {
+  const double dP = g.dP[c], Dz = g.Dz[c];
+  return (dP > 0.0 && Dz > 0.0) ? dP / (kGravity * Dz) : 1.0;
+}
+
+__device__ __forceinline__ double vl_phi(double up, double far, double down) {
+  const double num = up - far;
+  const double den = down - up;
+  const bool tiny = fabs(den) < 1e-30;
+  double r = num / (tiny ? 1e-30 : den);
+  if (tiny) r = fabs(num) < 1e-30 ? 1.0 : 1e6;
+  return (r + fabs(r)) / (1.0 + fabs(r));
+}
+
+__device__ __forceinline__ double dx_at(const orbit_met_t& g, int j) {
+  return kEarthRadius * cos(g.lat[j] * kDegToRad) * g.dlon * kDegToRad;
+}
+
+// Face between lo = (k, j, i-1) [x] or (k, j-1, i) [y] and hi = cell index `hi`.
+// Returns flux = A * inv and the terrain weights; valid flag.
+struct Face {
+  double flux, trL, trR;
+  bool ok;
+};
+
+__device__ Face x_face(const FctGeom& G, const double* x, int k, int j, int ihi) {
+  const orbit_met_t& g = G.g;
+  const int nx = G.nx;
+  const int64_t base = ((int64_t)k * G.ny + j) * nx;
+  const int64_t hi = base + ihi, lo = hi - 1;
+  const double cL = x[lo], cR = x[hi];
+  const double cLL = ihi - 1 > 0 ? x[lo - 1] : cL;
+  const double cRR = ihi < nx - 1 ? x[hi + 1] : cR;
+  double pL = vl_phi(cL, cLL, cR);
+  double pR = vl_phi(cR, cRR, cL);
+  if (ihi - 1 == 0) pL = 0.0;
+  if (ihi == nx - 1) pR = 0.0;
+  const double up = G.g.split ? g.u_plus[hi] : fmax(g.u[hi], 0.0);
+  const double um = G.g.split ? g.u_minus[hi] : fmax(-g.u[hi], 0.0);
+  const double beta = 0.5 * (up * pL + um * pR);
+  const double A = beta * (cR - cL);
+  const double d = dx_at(g, j);
+  const double inv = 1.0 / (d > 0.0 ? d : 1.0);
+  const double dl = g.dP[lo], dr = g.dP[hi];
+  Face f;
+  f.ok = dl > 0.0 && dr > 0.0;
+  const double face = 0.5 * (dl + dr);
+  f.trL = f.ok ? face / (dl > 0.0 ? dl : 1.0) : 1.0;
+  f.trR = f.ok ? face / (dr > 0.0 ? dr : 1.0) : 1.0;
+  f.flux = A * inv;
+  return f;
+}
+
+__device__ Face y_face(const FctGeom& G, const double* x, int k, int jhi, int i) {
+  const orbit_met_t& g = G.g;
+  const int nx = G.nx, ny = G.ny;
+  const int64_t hi = ((int64_t)k * ny + jhi) * nx + i, lo = hi - nx;
+  const double cS = x[lo], cN = x[hi];
+  const double cSS = jhi - 1 > 0 ? x[lo - nx] : cS;
+  const double cNN = jhi < ny - 1 ? x[hi + nx] : cN;
+  double pS = vl_phi(cS, cSS, cN);
+  double pN = vl_phi(cN, cNN, cS);
+  if (jhi - 1 == 0) pS = 0.0;
+  if (jhi == ny - 1) pN = 0.0;
+  const double vp = G.g.split ? g.v_plus[hi] : fmax(g.v[hi], 0.0);
+  const double vm = G.g.split ? g.v_minus[hi] : fmax(-g.v[hi], 0.0);
+  const double beta = 0.5 * (vp * pS + vm * pN);
+  const double A = beta * (cN - cS);
+  const double dy = kEarthRadius * g.dlat * kDegToRad;
+  const double inv = 1.0 / (dy > 0.0 ? dy : 1.0);
+  const double dxs = dx_at(g, jhi - 1), dxn = dx_at(g, jhi);
+  const double dxf = 0.5 * (dxs + dxn);
+  const double ds = g.dP[lo], dn = g.dP[hi];
+  Face f;
+  f.ok = ds > 0.0 && dn > 0.0;
+  const double face = 0.5 * (ds + dn);
+  f.trL = f.ok ? (dxf / (dxs > 0.0 ? dxs : 1.0)) * (face / (ds > 0.0 ? ds : 1.0)) : 1.0;
+  f.trR = f.ok ? (dxf / (dxn > 0.0 ? dxn : 1.0)) * (face / (dn > 0.0 ? dn : 1.0)) : 1.0;
+  f.flux = A * inv;
+  return f;
+}
+
+// x = c / rho for all vectors
+__global__ void k_fct_x(FctGeom G, const double* c, double* x, int64_t N) {
+  const double* cv = c + (int64_t)blockIdx.y * N;
+  double* xv = x + (int64_t)blockIdx.y * N;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (int64_t)gridDim.x * blockDim.x)
+    xv[e] = cv[e] / rho_at(G.g, e);
+}
+
+__global__ void k_fct_ratio(FctGeom G, const double* x_all, double* Rp_all, double* Rm_all, int64_t N) {
+  const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= N) return;
+  const double* x = x_all + (int64_t)blockIdx.y * N;
+  const int nx = G.nx, ny = G.ny;
+  const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
+  const double c = x[cell];
+  double cmax = c, cmin = c;
+  const double w = i > 0 ? x[cell - 1] : c, e = i < nx - 1 ? x[cell + 1] : c;
+  const double s = j > 0 ? x[cell - nx] : c, n = j < ny - 1 ? x[cell + nx] : c;
+  cmax = fmax(fmax(fmax(cmax, w), fmax(e, s)), n);
+  cmin = fmin(fmin(fmin(cmin, w), fmin(e, s)), n);
+  double Pp = 0.0, Pm = 0.0;
+  auto acc = [&](double into) {
+    Pp += fmax(into, 0.0);
+    Pm += fmax(-into, 0.0);
+  };
+  if (nx > 1) {
+    if (i > 0) {
+      Face f = x_face(G, x, k, j, i);
+      acc(f.ok ? f.trR * f.flux : 0.0);
+    }
+    if (i < nx - 1) {
+      Face f = x_face(G, x, k, j, i + 1);
+      acc(f.ok ? -f.trL * f.flux : 0.0);
+    }
+  }
+  if (ny > 1) {
+    if (j > 0) {
+      Face f = y_face(G, x, k, j, i);
+      acc(f.ok ? f.trR * f.flux : 0.0);
+    }
+    if (j < ny - 1) {
+      Face f = y_face(G, x, k, j + 1, i);
+      acc(f.ok ? -f.trL * f.flux : 0.0);
+    }
+  }
+  const double Qp = (cmax - c) / G.dt, Qm = (c - cmin) / G.dt;
+  Rp_all[(int64_t)blockIdx.y * N + cell] = Pp > 0.0 ? fmin(1.0, Qp / Pp) : 0.0;
+  Rm_all[(int64_t)blockIdx.y * N + cell] = Pm > 0.0 ? fmin(1.0, Qm / Pm) : 0.0;
+}
+
+__global__ void k_fct_div(FctGeom G, const double* x_all, const double* Rp_all, const double* Rm_all,
+                          int limited, double* d_all, int64_t N) {
+  const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= N) return;
+  const double* x = x_all + (int64_t)blockIdx.y * N;
+  const double* Rp = Rp_all + (int64_t)blockIdx.y * N;
+  const double* Rm = Rm_all + (int64_t)blockIdx.y * N;
+  const int nx = G.nx, ny = G.ny;
+  const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
+  auto limiter = [&](const Face& f, int64_t lo, int64_t hi) {
+    if (!limited) return 1.0;
+    const double into_hi = f.ok ? f.trR * f.flux : 0.0;
+    double C = into_hi >= 0.0 ? fmin(Rp[hi], Rm[lo]) : fmin(Rm[hi], Rp[lo]);
+    return fmin(fmax(C, 0.0), 1.0);
+  };
+  double d = 0.0;
+  if (nx > 1) {
+    if (i > 0) {
+      Face f = x_face(G, x, k, j, i);
+      const double fl = limiter(f, cell - 1, cell) * f.flux;
+      d += f.ok ? f.trR * fl : 0.0;
+    }
+    if (i < nx - 1) {
+      Face f = x_face(G, x, k, j, i + 1);
+      const double fl = limiter(f, cell, cell + 1) * f.flux;
+      d -= f.ok ? f.trL * fl : 0.0;
+    }
+  }
+  if (ny > 1) {
+    if (j > 0) {
+      Face f = y_face(G, x, k, j, i);
+      const double fl = limiter(f, cell - nx, cell) * f.flux;
+      d += f.ok ? f.trR * fl : 0.0;
+    }
+    if (j < ny - 1) {
+      Face f = y_face(G, x, k, j + 1, i);
+      const double fl = limiter(f, cell, cell + nx) * f.flux;
+      d -= f.ok ? f.trL * fl : 0.0;
+    }
+  }
+  d_all[(int64_t)blockIdx.y * N + cell] = d * rho_at(G.g, cell);
+}
+
+}  // namespace
+
+int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
+               int limited, double* d, double* scratch, cudaStream_t st) {
+  const int64_t N = (int64_t)nz * ny * nx;
+  FctGeom G{*met, nz, ny, nx, dt};
+  double* x = scratch;
+  double* Rp = scratch + (int64_t)n_vec * N;
+  double* Rm = Rp + (int64_t)n_vec * N;
+  dim3 g((unsigned)((N + 127) / 128), n_vec);
+  k_fct_x<<<g, 128, 0, st>>>(G, c, x, N);
+  if (limited) k_fct_ratio<<<g, 128, 0, st>>>(G, x, Rp, Rm, N);
+  k_fct_div<<<g, 128, 0, st>>>(G, x, Rp, Rm, limited, d, N);
+  ORBIT_CUDA_TRY(cudaGetLastError());
+  return ORBIT_OK;
+}
+
+}  // namespace orbit

@@ -1,0 +1,399 @@
+// Geometric nested dissection + dense-supernode symbolic analysis.
+//
+// The reference factors each I + dtau L_tau with UMFPACK (or SuperLU) behind
+// a fill-reducing ordering computed once per run (COLAMD, or METIS nested
+// dissection through pymetis; orbit/core/solve.py:88-207,299-335).  The
+// operator here is a 7-point stencil on a logically rectangular (nz, ny, nx)
+// grid, so the ordering is computed geometrically: the box is cut recursively
+// through its longest dimension by a one-cell-thick plane until a box holds at
+// most `leaf_cells` cells.  Every plane (and every leaf box) is one supernode;
+// its unknowns are eliminated after both half-boxes, and after elimination it
+// is coupled densely to exactly the cells of ancestor planes that touch its box
+// (the 6-neighbours of the box), which gives the multifrontal update sets
+// without any graph search.
+#include "symbolic.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <functional>
+
+namespace orbit {
+
+namespace {
+
+struct Box {
+  int lo[3], hi[3];  // [k, j, i]
+  int64_t cells() const {
+    return int64_t(hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+  }
+};
+
+struct Node {
+  Box box;      // region of the subtree
+  Box own;      // own cells (separator plane or the leaf box)
+  int c[2] = {-1, -1};
+  int parent = -1;
+  int depth = 0;
+};
+
+}  // namespace
+
+std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_elems,
+                           Symbolic& S) {
+  if (nz < 1 || ny < 1 || nx < 1) return "grid dimensions must be positive";
+  if (int64_t(nz) * ny * nx > (int64_t(1) << 30)) return "grid too large";
+  if (leaf_cells < 1) leaf_cells = 1;
+  if (chunk_elems < 256) chunk_elems = 256;
+  S = Symbolic();
+  S.nz = nz; S.ny = ny; S.nx = nx;
+  S.N = int64_t(nz) * ny * nx;
+  S.leaf_cells = leaf_cells;
+  const int64_t N = S.N;
+  const int dims[3] = {nz, ny, nx};
+
+  // ---- recursive dissection (explicit stack, postorder numbering) ----
+  std::vector<Node> nodes;
+  std::function<int(const Box&, int, int)> rec = [&](const Box& b, int depth, int par) -> int {
+    Node nd;
+    nd.box = b;
+    nd.depth = depth;
+    nd.parent = par;
+    int ext[3] = {b.hi[0] - b.lo[0], b.hi[1] - b.lo[1], b.hi[2] - b.lo[2]};
+    int kids[2] = {-1, -1};
+    if (b.cells() <= leaf_cells || (ext[0] <= 1 && ext[1] <= 1 && ext[2] <= 1)) {
+      nd.own = b;
+    } else {
+      // longest dimension; ties prefer the horizontal axes (x, then y)
+      int a = 2;
+      if (ext[1] > ext[a]) a = 1;
+      if (ext[0] > ext[a]) a = 0;
+      int mid = (b.lo[a] + b.hi[a]) / 2;
+      Box sep = b; sep.lo[a] = mid; sep.hi[a] = mid + 1;
+      Box c1 = b; c1.hi[a] = mid;
+      Box c2 = b; c2.lo[a] = mid + 1;
+      nd.own = sep;
+      int slot = 0;
+      // children first (postorder), recorded after the recursion
+      int self_placeholder = -1;
+      (void)self_placeholder;
+      std::vector<Box> cb;
+      if (c1.hi[a] > c1.lo[a]) cb.push_back(c1);
+      if (c2.hi[a] > c2.lo[a]) cb.push_back(c2);
+      for (auto& cbx : cb) kids[slot++] = rec(cbx, depth + 1, -2);
+    }
+    nd.c[0] = kids[0];
+    nd.c[1] = kids[1];
+    nodes.push_back(nd);
+    int id = int(nodes.size()) - 1;
+    for (int q = 0; q < 2; ++q)
+      if (kids[q] >= 0) nodes[kids[q]].parent = id;
+    return id;
+  };
+  Box root{{0, 0, 0}, {nz, ny, nx}};
+  rec(root, 0, -1);
+  const int ns = int(nodes.size());
+  S.nsuper = ns;
+
+  // ---- numbering ----
+  S.perm.assign(N, -1);
+  S.iperm.assign(N, -1);
+  S.first.resize(ns); S.n.resize(ns); S.m.resize(ns); S.parent.resize(ns);
+  S.level.resize(ns); S.nchild.resize(ns); S.child.assign(2 * ns, -1);
+  int64_t next = 0;
+  for (int s = 0; s < ns; ++s) {
+    const Node& nd = nodes[s];
+    S.first[s] = int32_t(next);
+    const Box& o = nd.own;
+    for (int k = o.lo[0]; k < o.hi[0]; ++k)
+      for (int j = o.lo[1]; j < o.hi[1]; ++j)
+        for (int i = o.lo[2]; i < o.hi[2]; ++i) {
+          int64_t cell = (int64_t(k) * ny + j) * nx + i;
+          S.perm[next] = int32_t(cell);
+          S.iperm[cell] = int32_t(next);
+          ++next;
+        }
+    S.n[s] = int32_t(next - S.first[s]);
+    S.parent[s] = nd.parent;
+    S.level[s] = nd.depth;
+    S.nchild[s] = (nd.c[0] >= 0) + (nd.c[1] >= 0);
+    S.child[2 * s] = nd.c[0];
+    S.child[2 * s + 1] = nd.c[1];
+  }
+  if (next != N) return "internal: numbering does not cover the grid";
+  S.sup_of.resize(N);
+  for (int s = 0; s < ns; ++s)
+    for (int q = 0; q < S.n[s]; ++q) S.sup_of[S.first[s] + q] = s;
+  // first index of each subtree (postorder => contiguous range)
+  std::vector<int32_t> sub_first(ns);
+  for (int s = 0; s < ns; ++s) {
+    int32_t f = S.first[s];
+    for (int q = 0; q < 2; ++q)
+      if (nodes[s].c[q] >= 0) f = std::min(f, sub_first[nodes[s].c[q]]);
+    sub_first[s] = f;
+  }
+
+  // ---- update sets: 6-neighbours of the subtree box ----
+  S.uoff.assign(ns + 1, 0);
+  std::vector<std::vector<int32_t>> U(ns);
+  for (int s = 0; s < ns; ++s) {
+    const Box& b = nodes[s].box;
+    std::vector<int32_t>& u = U[s];
+    for (int a = 0; a < 3; ++a)
+      for (int side = 0; side < 2; ++side) {
+        int plane = side == 0 ? b.lo[a] - 1 : b.hi[a];
+        if (plane < 0 || plane >= dims[a]) continue;
+        Box f = b;
+        f.lo[a] = plane;
+        f.hi[a] = plane + 1;
+        for (int k = f.lo[0]; k < f.hi[0]; ++k)
+          for (int j = f.lo[1]; j < f.hi[1]; ++j)
+            for (int i = f.lo[2]; i < f.hi[2]; ++i) {
+              int64_t cell = (int64_t(k) * ny + j) * nx + i;
+              u.push_back(S.iperm[cell]);
+            }
+      }
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    int32_t last = S.first[s] + S.n[s];
+    for (int32_t x : u)
+      if (x < last) return "internal: update set reaches a non-ancestor";
+    S.m[s] = int32_t(u.size());
+    S.uoff[s + 1] = S.uoff[s] + int64_t(u.size());
+  }
+  S.uidx.resize(S.uoff[ns]);
+  S.rel.resize(S.uoff[ns]);
+  for (int s = 0; s < ns; ++s) {
+    std::copy(U[s].begin(), U[s].end(), S.uidx.begin() + S.uoff[s]);
+    int p = S.parent[s];
+    for (size_t q = 0; q < U[s].size(); ++q) {
+      int32_t x = U[s][q];
+      int32_t pos = -1;
+      if (p < 0) return "internal: root has a non-empty update set";
+      if (x >= S.first[p] && x < S.first[p] + S.n[p]) {
+        pos = x - S.first[p];
+      } else {
+        auto it = std::lower_bound(U[p].begin(), U[p].end(), x);
+        if (it == U[p].end() || *it != x) return "internal: update set not inside the parent front";
+        pos = S.n[p] + int32_t(it - U[p].begin());
+      }
+      S.rel[S.uoff[s] + q] = pos;
+    }
+  }
+
+  // ---- levels, storage ----
+  int maxd = 0;
+  for (int s = 0; s < ns; ++s) maxd = std::max(maxd, S.level[s]);
+  S.nlevels = maxd + 1;
+  S.level_sups.assign(S.nlevels, {});
+  for (int s = 0; s < ns; ++s) S.level_sups[S.level[s]].push_back(s);
+  S.ldn.resize(ns); S.ldm.resize(ns); S.ldf.resize(ns);
+  S.fac_off.resize(ns); S.front_off.resize(ns); S.woff.resize(ns);
+  S.level_front_size.assign(S.nlevels, 0);
+  int64_t fo = 0, wo = 0;
+  double flops = 0.0;
+  for (int s = 0; s < ns; ++s) {
+    int64_t n = S.n[s], m = S.m[s];
+    S.ldn[s] = int32_t(round_up(n, kPad));
+    S.ldm[s] = int32_t(round_up(std::max<int64_t>(m, 1), kPad));
+    S.ldf[s] = int32_t(round_up(n + m, kPad));
+    S.fac_off[s] = fo;
+    fo += (n + m) * S.ldn[s] + n * S.ldm[s];
+    S.fac_nnz += n * n + 2 * n * m;
+    S.woff[s] = wo;
+    wo += m;
+    int l = S.level[s];
+    S.front_off[s] = S.level_front_size[l];
+    S.level_front_size[l] += (n + m) * S.ldf[s];
+    S.max_front = std::max<int>(S.max_front, int(n + m));
+    S.max_nm = std::max<int>(S.max_nm, int(std::max(n, m)));
+    double nn = double(n), mm = double(m);
+    flops += (2.0 / 3.0) * (std::pow(nn + mm, 3) - std::pow(mm, 3)) + (2.0 / 3.0) * nn * nn * nn +
+             2.0 * mm * nn * nn;
+  }
+  S.factor_flops = flops;
+  S.fac_size = fo;
+  S.w_size = std::max<int64_t>(wo, 1);
+  for (int l = 0; l < S.nlevels; ++l) S.front_buf_size = std::max(S.front_buf_size, S.level_front_size[l]);
+
+  // ---- original-entry scatter lists (grouped by level) ----
+  // Entry (row p, col q) of the permuted matrix lives in the front of the
+  // supernode owning min(p, q).
+  auto local_pos = [&](int s, int32_t x) -> int32_t {
+    if (x >= S.first[s] && x < S.first[s] + S.n[s]) return x - S.first[s];
+    const int32_t* b = S.uidx.data() + S.uoff[s];
+    const int32_t* e = S.uidx.data() + S.uoff[s + 1];
+    const int32_t* it = std::lower_bound(b, e, x);
+    if (it == e || *it != x) return -1;
+    return S.n[s] + int32_t(it - b);
+  };
+  std::vector<std::vector<std::pair<int64_t, int32_t>>> ent(S.nlevels);
+  const int di[7] = {0, -1, 1, 0, 0, 0, 0};
+  const int dj[7] = {0, 0, 0, -1, 1, 0, 0};
+  const int dk[7] = {0, 0, 0, 0, 0, -1, 1};
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        int64_t cell = (int64_t(k) * ny + j) * nx + i;
+        for (int d = 0; d < 7; ++d) {
+          int kk = k + dk[d], jj = j + dj[d], ii = i + di[d];
+          if (kk < 0 || kk >= nz || jj < 0 || jj >= ny || ii < 0 || ii >= nx) continue;
+          int64_t nb = (int64_t(kk) * ny + jj) * nx + ii;
+          int32_t p = S.iperm[cell], q = S.iperm[nb];
+          int s = S.sup_of[std::min(p, q)];
+          int32_t lr = local_pos(s, p), lc = local_pos(s, q);
+          if (lr < 0 || lc < 0) return "internal: matrix entry outside its front";
+          ent[S.level[s]].push_back({S.front_off[s] + int64_t(lr) * S.ldf[s] + lc,
+                                     int32_t(d * N + cell)});
+        }
+      }
+  S.ent_level_off.assign(S.nlevels + 1, 0);
+  for (int l = 0; l < S.nlevels; ++l) {
+    std::sort(ent[l].begin(), ent[l].end());
+    S.ent_level_off[l + 1] = S.ent_level_off[l] + int64_t(ent[l].size());
+  }
+  S.ent_pos.reserve(S.ent_level_off[S.nlevels]);
+  S.ent_src.reserve(S.ent_level_off[S.nlevels]);
+  for (int l = 0; l < S.nlevels; ++l)
+    for (auto& pr : ent[l]) {
+      S.ent_pos.push_back(pr.first);
+      S.ent_src.push_back(pr.second);
+    }
+
+  // ---- factorization schedule ----
+  auto push_item = [&](int a, int b, int c, int d) {
+    S.fitems.push_back(a); S.fitems.push_back(b); S.fitems.push_back(c); S.fitems.push_back(d);
+  };
+  auto nitems = [&]() { return int64_t(S.fitems.size() / 4); };
+  for (int l = S.nlevels - 1; l >= 0; --l) {
+    const auto& sups = S.level_sups[l];
+    S.fsched.push_back({FactorLaunch::ZERO, l, 0, 0, S.level_front_size[l]});
+    S.fsched.push_back({FactorLaunch::SCATTER, l, 0, S.ent_level_off[l],
+                        S.ent_level_off[l + 1] - S.ent_level_off[l]});
+    for (int slot = 0; slot < 2; ++slot) {
+      int64_t off = nitems();
+      for (int s : sups) {
+        int c = S.child[2 * s + slot];
+        if (c < 0) continue;
+        int rows = S.m[c];
+        for (int rb = 0; rb * 32 < rows; ++rb) push_item(c, rb, 0, 0);
+      }
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::EXTEND, l, slot, off, nitems() - off});
+    }
+    int nmax = 0;
+    for (int s : sups) nmax = std::max(nmax, S.n[s]);
+    for (int p0 = 0; p0 < nmax; p0 += kNB) {
+      int64_t off = nitems();
+      for (int s : sups)
+        if (S.n[s] > p0) push_item(s, 0, 0, 0);
+      S.fsched.push_back({FactorLaunch::DIAG, l, p0, off, nitems() - off});
+      off = nitems();
+      for (int s : sups) {
+        if (S.n[s] <= p0) continue;
+        int nb = std::min(kNB, S.n[s] - p0);
+        int rest = S.n[s] + S.m[s] - (p0 + nb);
+        for (int ch = 0; ch * kTile < rest; ++ch) {
+          push_item(s, 0, ch, 0);
+          push_item(s, 1, ch, 0);
+        }
+      }
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::PANEL, l, p0, off, nitems() - off});
+      off = nitems();
+      for (int s : sups) {
+        if (S.n[s] <= p0) continue;
+        int nb = std::min(kNB, S.n[s] - p0);
+        int rest = S.n[s] + S.m[s] - (p0 + nb);
+        int nt = (rest + kTile - 1) / kTile;
+        for (int tr = 0; tr < nt; ++tr)
+          for (int tc = 0; tc < nt; ++tc) push_item(s, tr, tc, 0);
+      }
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::UPDATE, l, p0, off, nitems() - off});
+    }
+    // blocked triangular inverses: step t fills block row t of Linv and block column t of Uinv
+    int tmax = (nmax + kNB - 1) / kNB;
+    for (int t = 1; t < tmax; ++t) {
+      int64_t off = nitems();
+      for (int s : sups) {
+        int nbk = (S.n[s] + kNB - 1) / kNB;
+        if (nbk <= t) continue;
+        for (int j = 0; j < t; ++j) {
+          push_item(s, 0, j, t);
+          push_item(s, 1, j, t);
+        }
+      }
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::INV, l, t * kNB, off, nitems() - off});
+    }
+    int64_t off = nitems();
+    for (int s : sups) {
+      int tn = (S.n[s] + kTile - 1) / kTile, tm = (S.m[s] + kTile - 1) / kTile;
+      for (int a = 0; a < tm; ++a)
+        for (int b = 0; b < tn; ++b) push_item(s, 0, a, b);  // Pb tile (rows of m, cols of n)
+      for (int a = 0; a < tn; ++a)
+        for (int b = 0; b < tm; ++b) push_item(s, 1, a, b);  // Qr tile (rows of n, cols of m)
+    }
+    if (nitems() > off) S.fsched.push_back({FactorLaunch::PROD, l, 0, off, nitems() - off});
+  }
+
+  // ---- solve schedule ----
+  // Rows of a supernode are split into chunks of roughly `chunk_elems`
+  // matrix elements so that large separators spread over many CTAs.
+  S.nchunk_fwd.assign(ns, 0); S.nchunk_bwd.assign(ns, 0);
+  S.nchunk_fwdT.assign(ns, 0); S.nchunk_bwdT.assign(ns, 0);
+  auto chunk_rows = [&](int s, int kind, int rows, std::function<int64_t(int)> rowlen) {
+    int start = 0;
+    int cnt = 0;
+    int64_t acc = 0;
+    for (int r = 0; r < rows; ++r) {
+      acc += std::max<int64_t>(rowlen(r), 1) + 8;
+      bool last = (r == rows - 1);
+      if (acc >= chunk_elems || last || (r + 1 - start) >= 1024) {
+        S.sitems.push_back(s); S.sitems.push_back(start); S.sitems.push_back(r + 1);
+        S.sitems.push_back(kind);
+        start = r + 1;
+        acc = 0;
+        ++cnt;
+      }
+    }
+    return cnt;
+  };
+  // non-transposed: fwd levels deep->0, bwd levels 0->deep
+  S.phase_off.clear();
+  for (int l = S.nlevels - 1; l >= 0; --l) {
+    S.phase_off.push_back(int32_t(S.sitems.size() / 4));
+    for (int s : S.level_sups[l]) {
+      int n = S.n[s], m = S.m[s];
+      S.nchunk_fwd[s] = chunk_rows(s, 0, n + m, [n](int r) { return r < n ? int64_t(r) : int64_t(n); });
+    }
+  }
+  for (int l = 0; l < S.nlevels; ++l) {
+    S.phase_off.push_back(int32_t(S.sitems.size() / 4));
+    for (int s : S.level_sups[l]) {
+      int n = S.n[s], m = S.m[s];
+      S.nchunk_bwd[s] = chunk_rows(s, 1, n, [n, m](int r) { return int64_t(n - r + m); });
+    }
+  }
+  S.phase_off.push_back(int32_t(S.sitems.size() / 4));
+  S.items_per_bin = S.phase_off.back();
+  // transposed: fwdT levels deep->0 over output columns (n+m), bwdT levels 0->deep over n columns
+  int32_t base = S.items_per_bin;
+  S.phase_offT.clear();
+  for (int l = S.nlevels - 1; l >= 0; --l) {
+    S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
+    for (int s : S.level_sups[l]) {
+      int n = S.n[s], m = S.m[s];
+      S.nchunk_fwdT[s] = chunk_rows(s, 2, n + m, [n](int c) { return c < n ? int64_t(c + 1) : int64_t(n); });
+    }
+  }
+  for (int l = 0; l < S.nlevels; ++l) {
+    S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
+    for (int s : S.level_sups[l]) {
+      int n = S.n[s], m = S.m[s];
+      S.nchunk_bwdT[s] = chunk_rows(s, 3, n, [n, m](int c) { return int64_t(n - c + m); });
+    }
+  }
+  S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
+  S.items_per_binT = S.phase_offT.back();
+  return std::string();
+}
+
+}  // namespace orbit

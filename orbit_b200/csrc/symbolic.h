@@ -1,0 +1,90 @@
+// Host symbolic analysis for the 7-point operator I + dtau L on an
+// (nz, ny, nx) box: geometric nested dissection into dense supernodes, the
+// multifrontal extend-add maps, and the static launch schedules of the
+// numeric factorization and of the chained triangular solves.
+//
+// One symbolic serves every species, bin and met draw of a domain shape: the
+// matrix pattern is the full 7-point stencil (explicit zeros where a face
+// carries no flux), which is the pattern-reuse contract the reference relies
+// on when it hands one UMFPACK symbolic to every species
+// (orbit/core/solve.py:88-207, orbit/core/orbit.py:79-96).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace orbit {
+
+// Stencil directions of the 7-point operator; values live as
+// stencil[dir * N + cell], cell = k*ny*nx + j*nx + i (reference CellIndexer,
+// orbit/core/indexing.py:5-45).
+enum StencilDir { D_C = 0, D_W = 1, D_E = 2, D_S = 3, D_N = 4, D_B = 5, D_T = 6 };
+
+constexpr int kTile = 64;      // dense tile edge of the factorization kernels
+constexpr int kNB = 64;        // panel width of the blocked LU
+constexpr int kPad = 4;        // leading-dimension padding (elements)
+
+inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+// One kernel launch of the numeric factorization schedule.
+struct FactorLaunch {
+  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, INV, PROD } kind;
+  int level;
+  int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV)
+  int64_t item_off;  // offset into the item array (int4 units)
+  int64_t items;     // number of items (per instance)
+};
+
+struct Symbolic {
+  int nz = 0, ny = 0, nx = 0;
+  int64_t N = 0;
+  int leaf_cells = 0;
+  int nsuper = 0;
+  int nlevels = 0;
+  // permutation: perm[new] = old cell; iperm[old] = new
+  std::vector<int32_t> perm, iperm;
+  // per supernode (postorder = elimination order)
+  std::vector<int32_t> first, n, m, parent, level, nchild;
+  std::vector<int32_t> child;        // 2 per supernode (-1 = none)
+  std::vector<int64_t> uoff;         // offset into uidx/rel, size nsuper+1
+  std::vector<int32_t> uidx;         // ancestor unknowns (new index), sorted
+  std::vector<int32_t> rel;          // position of uidx[i] in the parent front
+  std::vector<int32_t> sup_of;       // new index -> owning supernode
+  // dense storage
+  std::vector<int32_t> ldn, ldm, ldf;     // leading dims (padded)
+  std::vector<int64_t> fac_off;           // factor block offset per supernode
+  int64_t fac_size = 0;                   // elements per factor instance
+  int64_t fac_nnz = 0;                    // structural nonzeros sum(n^2 + 2nm)
+  std::vector<int64_t> front_off;         // offset within its level buffer
+  std::vector<int64_t> level_front_size;  // elements per instance per level
+  int64_t front_buf_size = 0;             // max over levels of level_front_size
+  std::vector<int64_t> woff;              // update-vector offset per supernode
+  int64_t w_size = 0;
+  // per level: supernodes of that level
+  std::vector<std::vector<int32_t>> level_sups;
+  // original-entry scatter: per level, (front position, stencil index) pairs
+  std::vector<int64_t> ent_level_off;     // size nlevels+1
+  std::vector<int64_t> ent_pos;           // position within the front (row*ld+col) + front_off
+  std::vector<int32_t> ent_src;           // dir*N + cell
+  // factorization schedule; items are int4 {a,b,c,d}
+  std::vector<int32_t> fitems;            // 4 ints per item
+  std::vector<FactorLaunch> fsched;
+  // solve schedule (per bin, shared by all instances): items {s, r0, r1, kind}
+  // kinds: 0 fwd, 1 bwd, 2 fwdT, 3 bwdT
+  std::vector<int32_t> sitems;            // 4 ints per item
+  std::vector<int32_t> phase_off;         // non-transposed phases (2*nlevels+1 offsets)
+  std::vector<int32_t> phase_offT;        // transposed phases
+  int32_t items_per_bin = 0, items_per_binT = 0;
+  // per supernode number of chunks in each solve kind
+  std::vector<int32_t> nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT;
+  int max_front = 0;
+  int max_nm = 0;
+  double factor_flops = 0.0;
+};
+
+// Build the symbolic analysis.  Returns an empty string on success, an
+// error message otherwise.
+std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_elems,
+                           Symbolic& S);
+
+}  // namespace orbit

@@ -1,0 +1,220 @@
+"""Device-side objects over the C ABI: met fields, transport stencils, factor
+batches (chained solves, periodic-orbit GMRES), FCT source, mass balance.
+
+Device memory is torch CUDA tensors (plumbing only); every computation runs
+in liborbit_b200's sm_100a kernels on the tensor's stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .symbolic import Symbolic
+from .synthetic import MetBin, DTAU, N_BINS
+
+_MET_FIELDS = ("dP", "Dz", "u", "v", "u_plus", "u_minus", "v_plus", "v_minus", "u_e", "u_plus_e",
+               "v_n", "v_plus_n", "kxxyy", "kzz", "w_plus", "w_minus", "cmfmc", "kmu", "kmv", "lat")
+
+
+def _stream(device=None):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("orbit_b200 device path needs a CUDA device (no CPU fallback)")
+
+
+class MetDevice:
+    """One bin's meteorology resident on the device (fields as in MetBin)."""
+
+    def __init__(self, met: MetBin, device="cuda"):
+        _require_cuda()
+        self.nz, self.ny, self.nx = met.nz, met.ny, met.nx
+        self.N = met.N
+        self.split = bool(met.split)
+        self.dlat, self.dlon = float(met.dlat), float(met.dlon)
+        self.t = {}
+        for name in _MET_FIELDS:
+            a = getattr(met, name)
+            if name in ("kmu", "kmv") and met.split:
+                continue
+            if name == "cmfmc" and (a.size == 0 or not np.any(a)):
+                continue
+            self.t[name] = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
+        rho = met.rho().reshape(-1)
+        self.rho = torch.as_tensor(rho, device=device)
+        self.struct = _lib.MetT(**{k: _lib.ptr(self.t.get(k)) for k in _MET_FIELDS},
+                                dlat=self.dlat, dlon=self.dlon, split=int(self.split))
+
+
+def assemble_transport(met: MetDevice, with_rowsum: bool = False):
+    """K1: [7, N] concentration-form transport stencil (and pressure-form row sums)."""
+    T = torch.empty((7, met.N), dtype=torch.float64, device=met.rho.device)
+    rs = torch.empty(met.N, dtype=torch.float64, device=met.rho.device) if with_rowsum else None
+    _lib.check(_lib.lib().orbit_assemble_transport(met.nz, met.ny, met.nx, C.byref(met.struct),
+                                                   _lib.ptr(T), _lib.ptr(rs), _stream()))
+    return (T, rs) if with_rowsum else T
+
+
+def stencil_to_csr(T: np.ndarray, nz: int, ny: int, nx: int):
+    """Host helper: scipy CSR of a [7, N] stencil (boundary entries dropped)."""
+    import scipy.sparse as sp
+    N = nz * ny * nx
+    c = np.arange(N)
+    k, r = np.divmod(c, nx * ny)
+    j, i = np.divmod(r, nx)
+    off = [0, -1, 1, -nx, nx, -nx * ny, nx * ny]
+    ok = [np.ones(N, bool), i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1]
+    rows, cols, vals = [], [], []
+    for d in range(7):
+        m = ok[d]
+        rows.append(c[m]); cols.append(c[m] + off[d]); vals.append(T[d][m])
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                         shape=(N, N))
+
+
+def fct_source(met: MetDevice, c: torch.Tensor, dt: float = DTAU, limited: bool = True):
+    """K2: FCT deferred-correction source for one or more (N,) concentration vectors."""
+    c2 = c.reshape(-1, met.N).contiguous()
+    d = torch.empty_like(c2)
+    _lib.check(_lib.lib().orbit_fct_source(met.nz, met.ny, met.nx, C.byref(met.struct), c2.shape[0],
+                                           _lib.ptr(c2), float(dt), int(limited), _lib.ptr(d),
+                                           _stream()))
+    return d.reshape(c.shape)
+
+
+def mass_balance(mets: Sequence[MetDevice], stencils: Sequence[torch.Tensor]) -> dict:
+    """K7 row sums on the device, then the same order statistics the reference
+    reports (operator.py:598-652): median, p90, p99, max of the interior rows
+    and the top layer, per-layer p90."""
+    g = mets[0]
+    nz, ny, nx = g.nz, g.ny, g.nx
+    nb = len(mets)
+    dev = g.rho.device
+    oi = torch.empty((nb, nz - 1, ny - 2, nx - 2), dtype=torch.float64, device=dev)
+    ot = torch.empty((nb, ny - 2, nx - 2), dtype=torch.float64, device=dev)
+    Tp = _lib.ptr_array([_lib.ptr(t) for t in stencils])
+    Rp = _lib.ptr_array([_lib.ptr(m.rho) for m in mets])
+    _lib.check(_lib.lib().orbit_mass_balance_rows(nz, ny, nx, nb, Tp, Rp, _lib.ptr(oi), _lib.ptr(ot),
+                                                  _stream()))
+    ri = oi.reshape(-1)
+    rt = ot.reshape(-1)
+    q = torch.tensor([0.5, 0.9, 0.99], dtype=torch.float64, device=dev)
+    qi = torch.quantile(ri, q)
+    qt = torch.quantile(rt, q[:2])
+    per_layer = torch.cat([oi, ot[:, None]], dim=1)  # (nb, nz, ny-2, nx-2)
+    lp90 = torch.stack([torch.quantile(per_layer[:, k].reshape(-1), 0.9) for k in range(nz)])
+    return {
+        "interior_median": float(qi[0]), "interior_p90": float(qi[1]), "interior_p99": float(qi[2]),
+        "interior_max": float(ri.max()),
+        "interior_frac_above_0.01": float((ri > 0.01).double().mean()),
+        "interior_frac_above_0.1": float((ri > 0.1).double().mean()),
+        "top_median": float(qt[0]), "top_p90": float(qt[1]),
+        "layer_p90": [float(v) for v in lp90],
+    }
+
+
+class FactorBatch:
+    """n_orbits x 8 numeric factorizations sharing a Symbolic, plus the chained
+    solves and the periodic-orbit GMRES that run on them."""
+
+    def __init__(self, sym: Symbolic, n_orbits: int, precision: int = 64):
+        _require_cuda()
+        self.sym = sym
+        self.n_orbits = int(n_orbits)
+        self.precision = int(precision)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().orbit_factor_create(sym.handle, self.n_orbits, self.precision,
+                                                  C.byref(h)))
+        self._h = h
+        self.n_factored = 0
+        self.N = sym.N
+
+    def numeric(self, T_stencils: Sequence[torch.Tensor], sinks: Optional[Sequence[torch.Tensor]],
+                dtau: float = DTAU):
+        """Factor len(T_stencils)//8 orbits; lists are orbit-major, bin-minor."""
+        n_inst = len(T_stencils)
+        if n_inst % N_BINS or n_inst // N_BINS > self.n_orbits:
+            raise ValueError("need 8 stencils per orbit, at most n_orbits orbits")
+        tp = _lib.ptr_array([_lib.ptr(t) for t in T_stencils])
+        dp = _lib.ptr_array([_lib.ptr(d) for d in sinks]) if sinks is not None else None
+        _lib.check(_lib.lib().orbit_factor_numeric(self._h, n_inst // N_BINS, tp, dp, float(dtau),
+                                                   _stream()))
+        self.n_factored = n_inst // N_BINS
+        self.dtau = float(dtau)
+
+    def chain(self, x: torch.Tensor, trans: bool = False, tau0: int = 0, tau1: int = N_BINS,
+              forcing: Optional[torch.Tensor] = None, fscale: float = 1.0, refine: bool = True):
+        """x: (n, N) -> P_{tau1-1}...P_{tau0} x (or the transposed chain)."""
+        x = x.reshape(-1, self.N).contiguous()
+        n = x.shape[0]
+        out = torch.empty_like(x)
+        f = forcing.reshape(n, N_BINS, self.N).contiguous() if forcing is not None else None
+        _lib.check(_lib.lib().orbit_chain_apply(self._h, n, int(trans), int(tau0), int(tau1),
+                                                _lib.ptr(x), _lib.ptr(out), _lib.ptr(f), float(fscale),
+                                                int(refine), _stream()))
+        return out
+
+    def solve(self, e: torch.Tensor, c_warm: Optional[torch.Tensor] = None, tol: float = 1e-6,
+              maxiter: int = 200, restart: int = 30, dtau: float = DTAU):
+        """Periodic orbits of the first n orbits: e (n, 8, N) -> (orbit (n, 9, N), info (n, 8))."""
+        e = e.reshape(-1, N_BINS, self.N).contiguous()
+        n = e.shape[0]
+        out = torch.empty((n, N_BINS + 1, self.N), dtype=torch.float64, device=e.device)
+        info = np.zeros((n, 8))
+        w = c_warm.reshape(n, self.N).contiguous() if c_warm is not None else None
+        rc = _lib.lib().orbit_gmres_solve(self._h, n, _lib.ptr(e), float(dtau), _lib.ptr(w), float(tol),
+                                          int(maxiter), int(restart), _lib.ptr(out), info.ctypes.data,
+                                          _stream())
+        if rc == 6:  # non-convergence: the reference warns and returns (orbit.py:184-186)
+            print(f"    WARNING: GMRES did not converge for some orbits (iters={info[:, 0].tolist()})")
+        else:
+            _lib.check(rc)
+        return out, info
+
+    def solve_adjoint(self, R: torch.Tensor, lam_warm: Optional[torch.Tensor] = None,
+                      tol: float = 1e-6, maxiter: int = 200, restart: int = 30):
+        R = R.reshape(-1, N_BINS, self.N).contiguous()
+        n = R.shape[0]
+        out = torch.empty((n, N_BINS + 1, self.N), dtype=torch.float64, device=R.device)
+        info = np.zeros((n, 8))
+        w = lam_warm.reshape(n, self.N).contiguous() if lam_warm is not None else None
+        rc = _lib.lib().orbit_adjoint_gmres_solve(self._h, n, _lib.ptr(R), _lib.ptr(w), float(tol),
+                                                  int(maxiter), int(restart), _lib.ptr(out),
+                                                  info.ctypes.data, _stream())
+        if rc == 6:
+            print(f"    WARNING: adjoint GMRES did not converge (iters={info[:, 0].tolist()})")
+        else:
+            _lib.check(rc)
+        return out, info
+
+    def bytes(self):
+        a, b = C.c_int64(), C.c_int64()
+        _lib.check(_lib.lib().orbit_factor_bytes(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().orbit_factor_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+INFO_FIELDS = ("gmres_iters", "residual", "periodicity", "neg_frac", "converged", "s_norm",
+               "outer_refinements", "matvecs")
+
+
+def info_dict(row) -> dict:
+    d = {k: float(v) for k, v in zip(INFO_FIELDS, row)}
+    d["gmres_iters"] = int(d["gmres_iters"])
+    return d

@@ -1,0 +1,72 @@
+"""Symbolic analysis handle (host side).
+
+``Symbolic(nz, ny, nx)`` is the counterpart of the reference's
+``umfpack_symbolic(L)`` (orbit/core/solve.py:88-207): computed once per
+domain shape and reused for every species, bin and met draw.  Where the
+reference derives an ordering from a sample matrix's pattern (COLAMD, or
+METIS through pymetis), this analysis is geometric nested dissection of the
+(nz, ny, nx) box into dense supernodes; the pattern is the full 7-point
+stencil, so no sample matrix is needed.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+_INT64_ARRAYS = {"uoff", "fac_off", "front_off", "level_front_size", "ent_level_off", "ent_pos", "woff"}
+
+INFO_KEYS = ("N", "nsuper", "nlevels", "factor_nnz", "factor_elems", "front_elems", "max_front",
+             "factor_flops", "solve_items_per_bin", "update_len", "leaf_cells", "max_nm")
+
+
+class Symbolic:
+    def __init__(self, nz: int, ny: int, nx: int, leaf_cells: int = 0):
+        L = _lib.lib()
+        h = C.c_void_p()
+        _lib.check(L.orbit_symbolic_create(int(nz), int(ny), int(nx), int(leaf_cells), C.byref(h)))
+        self._h = h
+        self.nz, self.ny, self.nx = int(nz), int(ny), int(nx)
+        self.N = self.nz * self.ny * self.nx
+        buf = (C.c_int64 * 12)()
+        _lib.check(L.orbit_symbolic_info(h, buf, 12))
+        self.info = {k: int(buf[i]) for i, k in enumerate(INFO_KEYS)}
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    @property
+    def lunz(self) -> int:
+        """Structural nonzeros of one factor (sum over supernodes of n^2 + 2 n m)."""
+        return self.info["factor_nnz"]
+
+    def array(self, name: str) -> np.ndarray:
+        L = _lib.lib()
+        cnt = C.c_int64()
+        _lib.check(L.orbit_symbolic_array(self._h, name.encode(), None, 0, C.byref(cnt)))
+        dt = np.int64 if name in _INT64_ARRAYS else np.int32
+        out = np.empty(cnt.value, dtype=dt)
+        _lib.check(L.orbit_symbolic_array(self._h, name.encode(), out.ctypes.data, cnt.value,
+                                          C.byref(cnt)))
+        return out
+
+    def perm(self) -> np.ndarray:
+        return self.array("perm")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().orbit_symbolic_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

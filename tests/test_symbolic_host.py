@@ -1,0 +1,157 @@
+"""Host-side checks of the symbolic analysis (no GPU needed).
+
+The structure produced by the C++ nested dissection is verified directly
+(permutation, update sets, extend-add maps, entry scatter), and the dense
+supernodal algorithm the CUDA kernels implement is replayed in numpy on those
+arrays: fronts assembled from the 7-point stencil, partial LU, explicit
+triangular inverses, then the chained forward/backward and transposed
+sweeps.  The replay must reproduce scipy's sparse solves of A x = b and
+A^T x = b, which pins the ordering, the update sets and the solve algebra.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from orbit_b200.symbolic import Symbolic
+from orbit_b200 import synthetic
+from oracle import assembly
+
+
+def _stencil_of(A, nz, ny, nx):
+    """[7][N] stencil of a 7-point CSR matrix (centre, W, E, S, N, B, T)."""
+    N = nz * ny * nx
+    A = A.tocsr()
+    st = np.zeros((7, N))
+    off = [0, -1, 1, -nx, nx, -nx * ny, nx * ny]
+    for c in range(N):
+        k, r = divmod(c, nx * ny)
+        j, i = divmod(r, nx)
+        ok = [True, i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1]
+        for d in range(7):
+            if ok[d]:
+                st[d, c] = A[c, c + off[d]]
+    return st
+
+
+def _matrix(nz, ny, nx, seed=3):
+    rng = np.random.default_rng(seed)
+    g = synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=2000.0, rho_profile=True, cmfmc_frac=0.4)
+    T = assembly.transport_block(g)
+    d = rng.uniform(1e-6, 1e-4, nz * ny * nx)
+    L = assembly.species_operator(T, d)
+    return (sp.eye(nz * ny * nx) + 10800.0 * L).tocsr()
+
+
+def _replay(sym, stencil):
+    a = {k: sym.array(k) for k in ("perm", "first", "n", "m", "parent", "level", "child", "uoff",
+                                   "uidx", "rel", "ldf", "front_off", "level_front_size",
+                                   "ent_level_off", "ent_pos", "ent_src")}
+    ns = len(a["n"])
+    nlev = int(a["level"].max()) + 1
+    flat = stencil.reshape(-1)
+    fronts, fac = {}, {}
+    for lev in range(nlev - 1, -1, -1):
+        buf = np.zeros(a["level_front_size"][lev])
+        e0, e1 = a["ent_level_off"][lev], a["ent_level_off"][lev + 1]
+        buf[a["ent_pos"][e0:e1]] = flat[a["ent_src"][e0:e1]]
+        for s in np.nonzero(a["level"] == lev)[0]:
+            n, m, ld = int(a["n"][s]), int(a["m"][s]), int(a["ldf"][s])
+            F = buf[a["front_off"][s]:a["front_off"][s] + (n + m) * ld].reshape(n + m, ld)[:, :n + m].copy()
+            for c in a["child"][2 * s:2 * s + 2]:
+                if c < 0:
+                    continue
+                rel = a["rel"][a["uoff"][c]:a["uoff"][c + 1]]
+                F[np.ix_(rel, rel)] += fronts.pop(c)
+            F11, F12, F21, F22 = F[:n, :n], F[:n, n:], F[n:, :n], F[n:, n:]
+            Lw = np.eye(n)
+            U = F11.copy()
+            for k in range(n):  # unpivoted LU
+                Lw[k + 1:, k] = U[k + 1:, k] / U[k, k]
+                U[k + 1:, k:] -= np.outer(Lw[k + 1:, k], U[k, k:])
+            U = np.triu(U)
+            Li, Ui = np.linalg.inv(Lw), np.linalg.inv(U)
+            L21 = F21 @ Ui
+            U12 = Li @ F12
+            fronts[s] = F22 - L21 @ U12
+            fac[s] = (np.tril(Li, -1) + np.triu(Ui), -L21 @ Li, -Ui @ U12)
+    return a, fac
+
+
+def _solve(a, fac, b, trans):
+    ns = len(a["n"])
+    nlev = int(a["level"].max()) + 1
+    perm = a["perm"]
+    bp = b[perm]
+    y = np.zeros_like(bp)
+    x = np.zeros_like(bp)
+    W = {}
+    for lev in range(nlev - 1, -1, -1):
+        for s in np.nonzero(a["level"] == lev)[0]:
+            n, m, f0 = int(a["n"][s]), int(a["m"][s]), int(a["first"][s])
+            SQ, Pb, Qr = fac[s]
+            v = np.zeros(n + m)
+            v[:n] = bp[f0:f0 + n]
+            for c in a["child"][2 * s:2 * s + 2]:
+                if c >= 0:
+                    v[a["rel"][a["uoff"][c]:a["uoff"][c + 1]]] += W.pop(c)
+            if not trans:
+                y[f0:f0 + n] = v[:n] + np.tril(SQ, -1) @ v[:n]
+                W[s] = v[n:] + Pb @ v[:n]
+            else:
+                y[f0:f0 + n] = np.triu(SQ).T @ v[:n]
+                W[s] = v[n:] + Qr.T @ v[:n]
+    for lev in range(nlev):
+        for s in np.nonzero(a["level"] == lev)[0]:
+            n, m, f0 = int(a["n"][s]), int(a["m"][s]), int(a["first"][s])
+            SQ, Pb, Qr = fac[s]
+            xu = x[a["uidx"][a["uoff"][s]:a["uoff"][s + 1]]]
+            if not trans:
+                x[f0:f0 + n] = np.triu(SQ) @ y[f0:f0 + n] + Qr @ xu
+            else:
+                x[f0:f0 + n] = (np.tril(SQ, -1) + np.eye(n)).T @ y[f0:f0 + n] + Pb.T @ xu
+    out = np.empty_like(x)
+    out[perm] = x
+    return out
+
+
+@pytest.mark.parametrize("shape,leaf", [((3, 4, 5), 4), ((5, 7, 6), 16), ((4, 9, 11), 8)])
+def test_structure(shape, leaf):
+    sym = Symbolic(*shape, leaf_cells=leaf)
+    N = sym.N
+    perm = sym.array("perm")
+    assert sorted(perm.tolist()) == list(range(N))
+    n, m, first = sym.array("n"), sym.array("m"), sym.array("first")
+    assert n.sum() == N and first[0] == 0 and np.all(np.diff(first) == n[:-1])
+    par, uoff, uidx = sym.array("parent"), sym.array("uoff"), sym.array("uidx")
+    assert (par < 0).sum() == 1
+    for s in range(len(n)):
+        u = uidx[uoff[s]:uoff[s + 1]]
+        assert np.all(np.diff(u) > 0)
+        assert np.all(u >= first[s] + n[s])  # only later (ancestor) unknowns
+    assert sym.lunz == int((n.astype(np.int64) ** 2 + 2 * n.astype(np.int64) * m).sum())
+
+
+@pytest.mark.parametrize("shape,leaf", [((3, 4, 5), 4), ((5, 7, 6), 16), ((4, 9, 11), 8)])
+def test_replay_matches_sparse_solve(shape, leaf):
+    A = _matrix(*shape)
+    st = _stencil_of(A, *shape)
+    sym = Symbolic(*shape, leaf_cells=leaf)
+    a, fac = _replay(sym, st)
+    rng = np.random.default_rng(1)
+    b = rng.standard_normal(sym.N)
+    x = _solve(a, fac, b, trans=False)
+    xr = spla.spsolve(A.tocsc(), b)
+    assert np.abs(x - xr).max() <= 1e-11 * np.abs(xr).max()
+    xt = _solve(a, fac, b, trans=True)
+    xtr = spla.spsolve(A.T.tocsc(), b)
+    assert np.abs(xt - xtr).max() <= 1e-11 * np.abs(xtr).max()
+
+
+def test_config_shapes_fill():
+    """Fill of the geometric dissection at the benchmark shapes (vs AMD 1.30 M / 45.7 M)."""
+    s0 = Symbolic(15, 20, 24)
+    s1 = Symbolic(15, 72, 80)
+    assert s0.lunz < 2.5e6
+    assert s1.lunz < 60e6
+    assert s1.info["max_front"] < 2048
