@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark: periodic orbits per second on B200 (one JSON line on rank 0).
+
+Workload (per GPU, per step): one batch of 12 species orbits on an 80x72x15
+domain (86,400 cells, 8 diurnal bins of 3 h) — one met draw of the
+12-species x 12-draw batched workload; successive steps cycle through
+different met draws.  A step is the whole hot path for the batch: transport
+assembly of the 8 bins (K1), 96 numeric factorizations of I + dtau L (K3), and
+the batched periodic-orbit GMRES over the chained bin solves (K4/K5) to tol
+1e-8.  Headline ``value``: mixed precision (FP32 factors and solves, FP64
+refinement, FP64 Arnoldi), all 12 orbits in one batch, inputs resident in HBM.
+``e2e``: the same with the inputs copied from pinned host memory and the
+orbits copied back inside the timed region.  ``plain_fp64``: the FP64 drop-in
+solving the same orbits one at a time.  Inputs are seeded synthetic fields
+(the reference's real met archive is not available).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun); orbits are independent, so each
+rank solves its own batches (weak scaling); the only collectives are the
+timing barrier and the max-over-ranks of the elapsed time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NZ, NY, NX = 15, 72, 80
+N_SPECIES = 12
+TOL = 1e-8
+METRIC = "orbits/s at <=1e-6 rel err (mixed FP32/FP64, batched)"
+WORKLOAD = "12 species x met draws, 80x72x15 (86,400 cells), 8 bins, GMRES(30) tol 1e-8, factor+solve"
+
+
+def _env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """Per-launch DRAM traffic of the chain kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "k_chain_traffic.txt")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_orbit_bin:"):
+                    return float(line.split(":", 1)[1])
+    except Exception:
+        pass
+    return None
+
+
+class Clocks:
+    def __init__(self, idx):
+        self.idx = idx
+        self.proc = None
+        self.path = os.path.join("/tmp", f"orbit_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    mx = max(mx, float(parts[1]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _make_inputs(rank, n_draws, seed=2024):
+    from orbit_b200 import synthetic
+    mets = [synthetic.make_met(seed + 1000 * (rank * 64 + d), NZ, NY, NX, cmfmc_frac=0.3)
+            for d in range(n_draws)]
+    spc = [synthetic.make_species(seed + 17 + s, NZ, NY, NX) for s in range(N_SPECIES)]
+    sinks = [[s.sink_diag(met) for s in spc] for met in mets]  # [draw][species] (8, N)
+    emis = np.stack([s.emis for s in spc])  # (S, 8, N)
+    return mets, spc, sinks, emis
+
+
+def cpu_baseline_sample(met, spc, n_matvec):
+    """The oracle port (SuperLU COLAMD + the reference's GMRES driver) on a bounded
+    sample of the same workload: one bin's factorization and one 8-bin solve
+    sweep, extrapolated to a full orbit (8 factorizations, n_matvec sweeps)."""
+    from oracle import assembly, orbit as oorbit
+    d = spc[0].sink_diag(met)
+    L = assembly.species_operator(assembly.transport_block(met[0]), d[0])
+    t0 = time.perf_counter()
+    lu = oorbit.factor_one_bin(L)
+    tf = time.perf_counter() - t0
+    x = np.asarray(spc[0].emis[0]) * 1e4
+    t0 = time.perf_counter()
+    for _ in range(8):
+        x = lu.solve(x)
+    ts = (time.perf_counter() - t0) / 8
+    t_orbit = 8 * tf + n_matvec * 8 * ts
+    return {"value": 1.0 / t_orbit, "unit": "orbits/s", "cores": 1, "kind": "port",
+            "sample": (f"1 of 8 bin factorizations ({tf:.1f} s, SuperLU COLAMD, nnz(LU)={lu.nnz}) + "
+                       f"8 bin solves ({ts * 1e3:.0f} ms each) of species 0, extrapolated to one orbit "
+                       f"= 8 factorizations + {n_matvec} 8-bin sweeps ({t_orbit:.0f} s)")}
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU algorithm (oracle port: SciPy SuperLU + GMRES(30)) on
+    this workload: each step solves one orbit end to end, factoring its 8 bins
+    on all host threads (ORBIT_FACTOR_THREADS-style) then running the GMRES."""
+    if rank != 0:
+        return
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import assembly, orbit as oorbit
+    mets, spc, sinks, emis = _make_inputs(0, 1)
+    met = mets[0]
+    cores = os.cpu_count() or 1
+    Ts = [assembly.transport_block(g) for g in met]
+
+    def one_orbit(s):
+        d = sinks[0][s]
+        with ThreadPoolExecutor(max_workers=min(cores, 8)) as ex:
+            lus = list(ex.map(lambda t: oorbit.factor_one_bin(assembly.species_operator(Ts[t], d[t])),
+                              range(8)))
+        return oorbit.solve_orbit_one_species(lus, list(emis[s]), tol=TOL)
+
+    def warm_sample():
+        # untimed warm-up: one bin factor + solve on a small slice of the same workload
+        L = assembly.species_operator(Ts[0], sinks[0][0][0])
+        lu = oorbit.factor_one_bin(L)
+        lu.solve(np.ones(L.shape[0]))
+
+    for _ in range(max(0, min(args.warmup, 1))):
+        warm_sample()
+    times = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        one_orbit(k % N_SPECIES)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = args.steps / total
+    line = {"metric": METRIC, "value": v, "unit": "orbits/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD.replace("factor+solve", "factor+solve, one orbit per step")},
+            "cpu_baseline": {"value": v, "unit": "orbits/s", "cores": min(cores, 8), "kind": "port",
+                             "sample": "one full orbit per step: 8 SuperLU (COLAMD) bin factorizations "
+                                       f"on {min(cores, 8)} threads + the reference GMRES driver"},
+            "e2e": {"value": v, "unit": "orbits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--draws", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = _env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from orbit_b200 import device
+    from orbit_b200.symbolic import Symbolic
+
+    mets, spc, sinks_h, emis_h = _make_inputs(rank, args.draws)
+    sym = Symbolic(NZ, NY, NX)
+    # device-resident inputs
+    met_dev = [[device.MetDevice(g) for g in met] for met in mets]
+    sinks_d = [[torch.as_tensor(sinks_h[d][s], device="cuda") for s in range(N_SPECIES)]
+               for d in range(args.draws)]
+    E = torch.as_tensor(emis_h, device="cuda")
+    fb = device.FactorBatch(sym, N_SPECIES, args.precision)
+
+    def step(d, fbx=None, E_=None, sink_rows=None, mets_=None):
+        fbx = fbx or fb
+        mets_ = mets_ or met_dev[d]
+        T = [device.assemble_transport(m) for m in mets_]
+        sk = sink_rows if sink_rows is not None else sinks_d[d]
+        fbx.numeric([T[b] for s in range(N_SPECIES) for b in range(8)],
+                    [sk[s][b] for s in range(N_SPECIES) for b in range(8)])
+        return fbx.solve(E if E_ is None else E_, tol=TOL)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for w in range(args.warmup):
+        step(w % args.draws)
+    # accuracy of the mixed path against the FP64 path on the same batch (untimed)
+    err = None
+    if args.precision == 32:
+        orb32, _ = step(0)
+        fb64 = device.FactorBatch(sym, N_SPECIES, 64)
+        orb64, _ = step(0, fbx=fb64)
+        err = float(((orb32 - orb64).abs().amax(dim=(1, 2)) / orb64.abs().amax(dim=(1, 2))).max())
+        del fb64, orb64, orb32
+        torch.cuda.empty_cache()
+
+    # ---- timed: device-resident ----
+    clocks = Clocks(local)
+    fb.profile(1)
+    launches0 = device.kernel_launches()
+    barrier()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    lat = []
+    infos = []
+    for k in range(args.steps):
+        e_a = torch.cuda.Event(enable_timing=True)
+        e_b = torch.cuda.Event(enable_timing=True)
+        e_a.record()
+        _, info = step(k % args.draws)
+        e_b.record()
+        lat.append((e_a, e_b))
+        infos.append(info)
+    ev1.record()
+    barrier()
+    clk = clocks.stop()
+    launches = device.kernel_launches() - launches0
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    prof = fb.profile(2)
+    fb.profile(0)
+    lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
+    orbits = N_SPECIES * args.steps * world
+    value = orbits / (ms / 1e3)
+
+    # ---- timed: end to end from pinned host buffers ----
+    import copy
+    keys = list(met_dev[0][0].t.keys())
+    pinned = [[{k: torch.from_numpy(np.ascontiguousarray(getattr(g, k), dtype=np.float64)).pin_memory()
+                for k in keys} for g in met] for met in mets]
+    sinks_p = [torch.from_numpy(np.stack(sinks_h[d])).pin_memory() for d in range(args.draws)]
+    emis_p = torch.from_numpy(emis_h).pin_memory()
+    out_p = torch.empty((N_SPECIES, 9, sym.N), dtype=torch.float64).pin_memory()
+    dev_sinks = torch.empty((N_SPECIES, 8, sym.N), dtype=torch.float64, device="cuda")
+    dev_E = torch.empty_like(E)
+    h2d = sum(t.numel() * 8 for b in pinned[0] for t in b.values()) + sinks_p[0].numel() * 8 + emis_p.numel() * 8
+    d2h = out_p.numel() * 8
+    barrier()
+    ev2 = torch.cuda.Event(enable_timing=True)
+    ev3 = torch.cuda.Event(enable_timing=True)
+    ev2.record()
+    for k in range(args.steps):
+        d = k % args.draws
+        for b, m in enumerate(met_dev[d]):
+            for key in keys:
+                m.t[key].copy_(pinned[d][b][key], non_blocking=True)
+        dev_sinks.copy_(sinks_p[d], non_blocking=True)
+        dev_E.copy_(emis_p, non_blocking=True)
+        orb, _ = step(d, E_=dev_E, sink_rows=[[dev_sinks[s, b] for b in range(8)] for s in range(N_SPECIES)])
+        out_p.copy_(orb, non_blocking=True)
+    ev3.record()
+    barrier()
+    ms_e2e = max_over_ranks(ev2.elapsed_time(ev3))
+    e2e = {"value": orbits / (ms_e2e / 1e3), "unit": "orbits/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h)}
+
+    # ---- plain FP64 drop-in, one orbit at a time (untimed by the headline) ----
+    plain = None
+    if not args.no_plain:
+        fb1 = device.FactorBatch(sym, 1, 64)
+        times = []
+        for s in range(N_SPECIES):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            T = [device.assemble_transport(m) for m in met_dev[0]]
+            torch.cuda.synchronize()
+            a.record()
+            T = [device.assemble_transport(m) for m in met_dev[0]]
+            fb1.numeric(T, [sinks_d[0][s][bb] for bb in range(8)])
+            o1, i1 = fb1.solve(E[s:s + 1], tol=TOL)
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        plain = {"value": 1e3 * len(times) / sum(times), "unit": "orbits/s",
+                 "latency_ms_p50": float(np.percentile(times, 50)),
+                 "latency_ms_p99": float(np.percentile(times, 99))}
+        del fb1
+
+    # ---- roofline of the chained-solve kernel (K4) ----
+    peak, peak_kind = _peaks()
+    chain_ms_avg = prof["chain_ms"] / max(prof["chain_launches"], 1)
+    chain_bytes = prof["chain_bytes"] / max(prof["chain_launches"], 1)
+    achieved = chain_bytes / (chain_ms_avg * 1e-3) / 1e9 if chain_ms_avg > 0 else 0.0
+    vb = 4 if args.precision == 32 else 8
+    tr = _profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tr * chain_bytes / (sym.lunz * vb)) if tr else None,
+                "kernel": "k_chain", "algorithmic_bytes_per_launch": chain_bytes,
+                "avg_launch_ms": chain_ms_avg, "launches": prof["chain_launches"],
+                "factor_nnz_per_bin": sym.lunz}
+    factor = {"kernel_group": "numeric factorization (K3)",
+              "ms_per_step": prof["factor_ms"] / max(args.steps, 1),
+              "achieved_tflops": prof["factor_flops"] / (prof["factor_ms"] * 1e-3) / 1e12
+              if prof["factor_ms"] > 0 else None,
+              "flops_per_factor": sym.info["factor_flops"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nmv = int(np.median([r[7] for inf in infos for r in inf]))
+        cpu = cpu_baseline_sample(mets[0], spc, nmv)
+
+    if rank == 0:
+        it = [r[0] for inf in infos for r in inf]
+        line = {
+            "metric": METRIC, "value": value, "unit": "orbits/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == 32 else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "orbits_per_step_per_gpu": N_SPECIES,
+                       "met_draws": args.draws, "grid": [NZ, NY, NX], "tol": TOL,
+                       "precision": "fp32 factors + fp64 refinement" if args.precision == 32 else "fp64",
+                       "l2": "inputs and factors (>15 GB) exceed L2 each step", "parallelism": f"orbits x{world}"},
+            "e2e": e2e, "roofline": roofline, "factorization": factor, "cpu_baseline": cpu,
+            "clocks": clk, "gpu_launches": int(launches),
+            "latency_ms": {"batch_p50": float(np.percentile(lat_ms, 50)),
+                           "batch_p99": float(np.percentile(lat_ms, 99))},
+            "plain_fp64": plain,
+            "mixed_vs_plain": (value / world / plain["value"]) if plain else None,
+            "max_rel_err_vs_fp64": err,
+            "gmres_iters_median": float(np.median(it)) if it else None,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

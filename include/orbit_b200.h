@@ -47,6 +47,10 @@ typedef struct orbit_factor_s* orbit_factor_t;
 const char* orbit_last_error(void);
 /* Library version string. */
 const char* orbit_version(void);
+/* Number of CUDA kernels this library has launched since it was loaded.  No
+ * reference counterpart (the reference runs no device code); used to account
+ * for device work in benchmarks. */
+long long orbit_kernel_launches(void);
 
 /* Per-bin averaged meteorology on the device (each pointer nz*ny*nx doubles
  * unless noted).  Field meaning follows GridData, orbit/core/grid_data.py:19-215. */
@@ -139,6 +143,13 @@ int orbit_factor_destroy(orbit_factor_t f);
  * the call returns (stream-ordered). */
 int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_stencils,
                          const double* const* sink_diags, double dtau, orbit_stream_t stream);
+/* Per-launch timing of the chained-solve kernel and of numeric factorizations
+ * (CUDA events on the caller's stream).  mode 1: enable and reset; 0: disable
+ * and reset; 2: read into out[6] = {chain launches, chain ms, chain
+ * algorithmic bytes (factor values read), factor calls, factor ms, factor
+ * flops}.  Reading synchronizes the recorded events.  The reference reports
+ * t_factor/t_solve wall times per species (orbit/core/orbit.py:331-383). */
+int orbit_factor_profile(orbit_factor_t f, int mode, double* out);
 /* Device bytes held by the factor handle (reference: numeric_bytes, solve.py:233-236). */
 int orbit_factor_bytes(orbit_factor_t f, int64_t* numeric_bytes, int64_t* workspace_bytes);
 

@@ -271,6 +271,7 @@ int assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T
   const int64_t NN = (int64_t)nz * ny * nx;
   const int threads = 128;
   k_assemble<<<(unsigned)((NN + threads - 1) / threads), threads, 0, st>>>(nz, ny, nx, *met, T, rowsum);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }
@@ -280,6 +281,7 @@ int mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* Ts
   const int64_t per = (int64_t)nz * (ny - 2) * (nx - 2);
   dim3 g((unsigned)((per + 255) / 256), nbins);
   k_mass_rows<<<g, 256, 0, st>>>(nz, ny, nx, Tst, rho, out_int, out_top);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
@@ -14,6 +15,8 @@ namespace orbit {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+static std::atomic<long long> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int run_factor(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st);
 int launch_chain(orbit_factor_s* f, int B, const int* d_orbit_ids, int trans, int tau0, int tau1,
@@ -119,6 +122,57 @@ extern "C" {
 
 const char* orbit_last_error(void) { return g_last_error.c_str(); }
 const char* orbit_version(void) { return "orbit_b200 0.1 (sm_100a)"; }
+
+long long orbit_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int orbit_factor_profile(orbit_factor_t f, int mode, double* out) {
+  if (!f) {
+    set_last_error("null handle");
+    return ORBIT_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(f->mu);
+  auto drop = [](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v) {
+    for (auto& e : v) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    v.clear();
+  };
+  if (mode == 0 || mode == 1) {
+    drop(f->prof_chain);
+    drop(f->prof_factor);
+    f->prof_chain_bytes = 0.0;
+    f->prof_factor_flops = 0.0;
+    f->prof_on = mode == 1;
+    return ORBIT_OK;
+  }
+  if (!out) {
+    set_last_error("out is NULL");
+    return ORBIT_ERR_ARG;
+  }
+  auto total = [](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, double& ms) -> int {
+    ms = 0.0;
+    for (auto& e : v) {
+      ORBIT_CUDA_TRY(cudaEventSynchronize(e.second));
+      float t = 0.f;
+      ORBIT_CUDA_TRY(cudaEventElapsedTime(&t, e.first, e.second));
+      ms += t;
+    }
+    return ORBIT_OK;
+  };
+  double cms = 0.0, fms = 0.0;
+  int rc = total(f->prof_chain, cms);
+  if (rc) return rc;
+  rc = total(f->prof_factor, fms);
+  if (rc) return rc;
+  out[0] = (double)f->prof_chain.size();
+  out[1] = cms;
+  out[2] = f->prof_chain_bytes;
+  out[3] = (double)f->prof_factor.size();
+  out[4] = fms;
+  out[5] = f->prof_factor_flops;
+  return ORBIT_OK;
+}
 
 int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out) {
   if (!out) {
@@ -345,6 +399,7 @@ int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit
 int orbit_factor_destroy(orbit_factor_t f) {
   if (!f) return ORBIT_OK;
   cudaDeviceSynchronize();
+  orbit_factor_profile(f, 0, nullptr);
   free_all(f->allocs);
   if (f->h_status) cudaFreeHost(f->h_status);
   if (f->h_scal) cudaFreeHost(f->h_scal);
@@ -371,7 +426,18 @@ int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_
   ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Tptr, T_stencils, sizeof(double*) * n_active * 8, cudaMemcpyHostToDevice, st));
   ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Dptr, dp.data(), sizeof(double*) * n_active * 8, cudaMemcpyHostToDevice, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(int), st));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (f->prof_on) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+  }
   int rc = run_factor(f, n_active, dtau, st);
+  if (f->prof_on) {
+    cudaEventRecord(e1, st);
+    f->prof_factor.push_back({e0, e1});
+    f->prof_factor_flops += (double)n_active * 8 * f->sym->S.factor_flops;
+  }
   if (rc) return rc;
   ORBIT_CUDA_TRY(cudaMemcpyAsync(f->h_status, f->status, sizeof(int), cudaMemcpyDeviceToHost, st));
   ORBIT_CUDA_TRY(cudaStreamSynchronize(st));

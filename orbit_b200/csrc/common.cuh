@@ -9,6 +9,8 @@
 namespace orbit {
 
 void set_last_error(const std::string& msg);
+// Count of kernels this library has launched (all handles, all threads).
+void note_launch(int n = 1);
 
 #define ORBIT_CUDA_TRY(expr)                                                     \
   do {                                                                           \

@@ -444,6 +444,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   {
     dim3 g(clamp_grid((7 * S.N + 255) / 256), n_inst);
     k_copy_A<<<g, 256, 0, st>>>(f->A_stencil, f->d_Tptr, f->d_Dptr, 0, S.N, dtau);
+    note_launch();
     ORBIT_CUDA_TRY(cudaGetLastError());
   }
   for (int base = 0; base < n_inst; base += f->front_group) {
@@ -456,42 +457,50 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
         case FactorLaunch::ZERO: {
           dim3 g(clamp_grid((L.items + 255) / 256), G);
           k_zero<T><<<g, 256, 0, st>>>(cur, L.items, S.front_buf_size);
+          note_launch();
           break;
         }
         case FactorLaunch::SCATTER: {
           dim3 g(clamp_grid((L.items + 255) / 256), G);
           k_scatter<T><<<g, 256, 0, st>>>(cur, S.front_buf_size, sy->d.ent_pos, sy->d.ent_src,
                                           L.item_off, L.items, f->d_Tptr, f->d_Dptr, base, S.N, dtau);
+          note_launch();
           break;
         }
         case FactorLaunch::EXTEND: {
           dim3 g((unsigned)L.items, G);
           k_extend<T><<<g, kThreads, 0, st>>>(D, cur, chl, L.item_off);
+          note_launch();
           break;
         }
         case FactorLaunch::DIAG: {
           dim3 g((unsigned)L.items, G);
           k_diag<T><<<g, kThreads, sm_diag, st>>>(D, cur, factors, L.item_off, L.p0, base, f->status);
+          note_launch();
           break;
         }
         case FactorLaunch::PANEL: {
           dim3 g((unsigned)L.items, G);
           k_panel<T><<<g, kThreads, sm_gemm, st>>>(D, cur, factors, L.item_off, L.p0, base);
+          note_launch();
           break;
         }
         case FactorLaunch::UPDATE: {
           dim3 g((unsigned)L.items, G);
           k_update<T><<<g, kThreads, sm_gemm, st>>>(D, cur, L.item_off, L.p0);
+          note_launch();
           break;
         }
         case FactorLaunch::INV: {
           dim3 g((unsigned)L.items, G);
           k_inv<T><<<g, kThreads, sm_inv, st>>>(D, cur, factors, L.item_off, base);
+          note_launch();
           break;
         }
         case FactorLaunch::PROD: {
           dim3 g((unsigned)L.items, G);
           k_prod<T><<<g, kThreads, sm_gemm, st>>>(D, cur, factors, L.item_off, base);
+          note_launch();
           break;
         }
       }

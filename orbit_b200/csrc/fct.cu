@@ -212,8 +212,11 @@ int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const 
   double* Rm = Rp + (int64_t)n_vec * N;
   dim3 g((unsigned)((N + 127) / 128), n_vec);
   k_fct_x<<<g, 128, 0, st>>>(G, c, x, N);
+  note_launch();
   if (limited) k_fct_ratio<<<g, 128, 0, st>>>(G, x, Rp, Rm, N);
+  note_launch();
   k_fct_div<<<g, 128, 0, st>>>(G, x, Rp, Rm, limited, d, N);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }

@@ -318,7 +318,9 @@ int upload_ids(Ctx& c, const std::vector<int>& ids, int* d_ids) {
 int sqnorm(Ctx& c, const double* v, int64_t vstride, const int* d_ids, int B, int slot) {
   orbit_factor_s* f = c.f;
   k_multidot<<<dim3(kRedBlocks, B), kVT, 0, c.st>>>(c.partial, v, vstride, 1, v, vstride, d_ids, c.N);
+  note_launch();
   k_reduce_partials<<<B, 32, 0, c.st>>>(f->scal, kScal, slot, c.partial, 1, d_ids, 0);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }
@@ -361,17 +363,22 @@ int refined_bin(Ctx& c, const int* d_ids, int B, int tau, int tau1, const double
   Scal one{nullptr, 0, 0, 1.0}, fs{nullptr, 0, 0, fscale};
   // XS[bin_in] = b
   k_lincomb<<<g, kVT, 0, c.st>>>(XS + bin_in * N, xs, one, X + bin_in * N, xs, fs, Ein, 8 * N, d_ids, N);
+  note_launch();
   int rc = launch_chain_x(f, XS, B, d_ids, trans, tau, tau + 1, nullptr, 0.0, c.st);
   if (rc) return rc;
   // xhat -> Tv ; r = b - A xhat -> XS[bin_in]
   k_lincomb<<<g, kVT, 0, c.st>>>(c.Tv, c.vs, one, XS + bin_out * N, xs, one, nullptr, 0, d_ids, N);
+  note_launch();
   k_stencil_resid<<<g, kVT, 0, c.st>>>(c.Rv, c.vs, XS + bin_in * N, xs, c.Tv, c.vs, f->A_stencil, tau,
                                        sy->d.perm, sy->d.iperm, sy->S.nz, sy->S.ny, sy->S.nx, trans, d_ids);
+  note_launch();
   k_lincomb<<<g, kVT, 0, c.st>>>(XS + bin_in * N, xs, one, c.Rv, c.vs, one, nullptr, 0, d_ids, N);
+  note_launch();
   rc = launch_chain_x(f, XS, B, d_ids, trans, tau, tau + 1, nullptr, 0.0, c.st);
   if (rc) return rc;
   // X[bin_out] = xhat + correction
   k_lincomb<<<g, kVT, 0, c.st>>>(X + bin_out * N, xs, one, c.Tv, c.vs, one, XS + bin_out * N, xs, d_ids, N);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }
@@ -397,6 +404,7 @@ int chain_accurate(Ctx& c, const int* d_ids, int B, const double* E, double fsca
       Scal one{nullptr, 0, 0, 1.0}, fs{nullptr, 0, 0, fscale};
       k_lincomb<<<g, kVT, 0, c.st>>>(f->X + (int64_t)tau0 * c.N, 9 * c.N, one, f->X + (int64_t)tau0 * c.N,
                                      9 * c.N, fs, E + (int64_t)tau0 * c.N, 8 * c.N, d_ids, c.N);
+      note_launch();
     }
   }
   ORBIT_CUDA_TRY(cudaGetLastError());
@@ -412,10 +420,12 @@ int matvec(Ctx& c, const double* v, int64_t vstride, double* w, int64_t wstride,
   Scal one{nullptr, 0, 0, 1.0}, mone{nullptr, 0, 0, -1.0};
   const int in = c.trans ? 8 : 0, out = c.trans ? 0 : 8;
   k_lincomb<<<g, kVT, 0, c.st>>>(f->X + in * N, 9 * N, one, v, vstride, one, nullptr, 0, d_ids, N);
+  note_launch();
   int rc = (accurate && c.mixed) ? chain_accurate(c, d_ids, B, nullptr, 0.0)
                                  : launch_chain(f, B, d_ids, c.trans, 0, 8, nullptr, 0.0, c.st);
   if (rc) return rc;
   k_lincomb<<<g, kVT, 0, c.st>>>(w, wstride, one, v, vstride, mone, f->X + out * N, 9 * N, d_ids, N);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }
@@ -442,11 +452,13 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
   if (B == 0) return ORBIT_OK;
   if (x_is_zero) {
     k_lincomb<<<vgrid(N, B), kVT, 0, c.st>>>(V_of(0), vstr, one, b, c.vs, one, nullptr, 0, d_ids, N);
+    note_launch();
   } else {
     rc = matvec(c, x, c.vs, c.Rv, c.vs, d_ids, B, accurate_mv);
     if (rc) return rc;
     for (int o : act) matvecs[o]++;
     k_lincomb<<<vgrid(N, B), kVT, 0, c.st>>>(V_of(0), vstr, one, b, c.vs, mone, c.Rv, c.vs, d_ids, N);
+    note_launch();
   }
   rc = sqnorm(c, V_of(0), vstr, d_ids, B, S_NORM);
   if (rc) return rc;
@@ -468,7 +480,9 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
     if (rc) return rc;
     // V0 = r / ||r|| ; g = [||r||, 0, ...]
     k_init_g<<<(B + 63) / 64, 64, 0, c.st>>>(f->gv, f->scal, d_ids, B);
+    note_launch();
     k_scale_inv_norm<<<vgrid(N, B), kVT, 0, c.st>>>(V_of(0), vstr, f->scal, S_NORM, d_ids, N);
+    note_launch();
     std::vector<int> inner = act;
     for (int o : act) ncol_h[o] = 0;
     for (int col = 0; col < R && !inner.empty(); ++col) {
@@ -486,21 +500,28 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
       // CGS2
       for (int pass = 0; pass < 2; ++pass) {
         k_multidot<<<dim3(kRedBlocks, Bi), kVT, 0, c.st>>>(c.partial, f->V, vstr, col + 1, c.Rv, c.vs, d_ids, N);
+        note_launch();
         k_reduce_partials<<<Bi, 32, 0, c.st>>>(f->Hd, hld * 32, col * hld, c.partial, col + 1, d_ids, pass);
+        note_launch();
         // w -= V h (pass 0 uses the full h; pass 1 must use only the increment) -> use Tv copy of increment
         if (pass == 0) {
           k_combine<<<g, kVT, 0, c.st>>>(c.Rv, c.vs, f->V, vstr, f->Hd, hld * 32, col * hld, nullptr, col + 1,
                                          -1.0, d_ids, N);
+          note_launch();
         } else {
           // the second-pass increment is also kept apart (red) to subtract only it
           k_reduce_partials<<<Bi, 32, 0, c.st>>>(f->red, 33, 0, c.partial, col + 1, d_ids, 0);
+          note_launch();
           k_combine<<<g, kVT, 0, c.st>>>(c.Rv, c.vs, f->V, vstr, f->red, 33, 0, nullptr, col + 1, -1.0, d_ids, N);
+          note_launch();
         }
       }
       rc = sqnorm(c, c.Rv, c.vs, d_ids, Bi, S_NORM);
       if (rc) return rc;
       k_normalize<<<g, kVT, 0, c.st>>>(V_of(col + 1), c.Rv, vstr, c.vs, f->Hd, hld, col, f->scal, d_ids, N);
+      note_launch();
       k_givens<<<(Bi + 63) / 64, 64, 0, c.st>>>(f->Hd, hld, f->cs, f->sn, f->gv, col, f->scal, d_ids, Bi);
+      note_launch();
       ORBIT_CUDA_TRY(cudaGetLastError());
       rc = fetch_scal(c);
       if (rc) return rc;
@@ -520,12 +541,15 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
     if (rc) return rc;
     ORBIT_CUDA_TRY(cudaMemcpyAsync(d_ncol, ncol_h.data(), sizeof(int) * f->n_orbits, cudaMemcpyHostToDevice, c.st));
     k_ysolve<<<(B + 63) / 64, 64, 0, c.st>>>(f->Hd, hld, f->gv, f->red, d_ncol, d_ids, B);
+    note_launch();
     k_combine<<<vgrid(N, B), kVT, 0, c.st>>>(x, c.vs, f->V, vstr, f->red, 33, 0, d_ncol, 0, 1.0, d_ids, N);
+    note_launch();
     // true residual r = b - A x -> V0 (unnormalised) and its norm
     rc = matvec(c, x, c.vs, c.Rv, c.vs, d_ids, B, accurate_mv);
     if (rc) return rc;
     for (int o : act) matvecs[o]++;
     k_lincomb<<<vgrid(N, B), kVT, 0, c.st>>>(V_of(0), vstr, one, b, c.vs, mone, c.Rv, c.vs, d_ids, N);
+    note_launch();
     rc = sqnorm(c, V_of(0), vstr, d_ids, B, S_NORM);
     if (rc) return rc;
     rc = fetch_scal(c);
@@ -568,6 +592,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   const dim3 g = vgrid(N, n);
   // forcing in permuted order
   k_perm_gather<<<g, kVT, 0, st>>>(f->E, 8 * N, e_or_R, 8 * N, 8, sy->d.perm, d_ids, N);
+  note_launch();
   // s: forward x0 = 0, P_tau(x + dtau e); adjoint x8 = 0, P^T x + R
   Scal one{nullptr, 0, 0, 1.0}, zero{nullptr, 0, 0, 0.0};
   const int in = trans ? 8 : 0, outb = trans ? 0 : 8;
@@ -579,6 +604,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   if (rc) return rc;
   for (int o = 0; o < n; ++o) mv[o]++;
   k_lincomb<<<g, kVT, 0, st>>>(c.Sv, c.vs, one, f->X + outb * N, 9 * N, zero, nullptr, 0, d_ids, N);
+  note_launch();
   rc = sqnorm(c, c.Sv, c.vs, d_ids, n, S_SN);
   if (rc) return rc;
   rc = fetch_scal(c);
@@ -598,8 +624,10 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   // x0 = warm or s
   if (warm) {
     k_perm_gather<<<g, kVT, 0, st>>>(c.Xv, c.vs, warm, N, 1, sy->d.perm, d_ids, N);
+    note_launch();
   } else {
     k_lincomb<<<g, kVT, 0, st>>>(c.Xv, c.vs, one, c.Sv, c.vs, zero, nullptr, 0, d_ids, N);
+    note_launch();
   }
   if (!c.mixed) {
     rc = gmres(c, act, c.Sv, c.Xv, atol, maxiter, false, iters, conv, rn, mv, false);
@@ -619,6 +647,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
       for (int o : oact) mv[o] += 2;
       Scal mone{nullptr, 0, 0, -1.0};
       k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, c.Sv, c.vs, mone, c.Rv, c.vs, d_ids, N);
+      note_launch();
       rc = sqnorm(c, c.Dv, c.vs, d_ids, B, S_TMP);
       if (rc) return rc;
       rc = fetch_scal(c);
@@ -646,11 +675,13 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
       std::vector<double> rin(f->n_orbits, 0.0);
       double* xcorr = f->tmpv + 5 * N;  // spare slot 5 of tmpv
       k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(xcorr, c.vs, zero, nullptr, 0, zero, nullptr, 0, d_ids, N);
+      note_launch();
       rc = gmres(c, oact, c.Dv, xcorr, itol, maxiter, false, iters, cin, rin, mv, true);
       if (rc) return rc;
       rc = upload_ids(c, oact, d_ids);
       if (rc) return rc;
       k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(c.Xv, c.vs, one, c.Xv, c.vs, one, xcorr, c.vs, d_ids, N);
+      note_launch();
       for (int o : oact) outer[o]++;
     }
   }
@@ -659,6 +690,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   if (rc) return rc;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * n, st));
   k_lincomb<<<g, kVT, 0, st>>>(f->X + in * N, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
+  note_launch();
   if (!trans) {
     rc = chain_accurate(c, d_ids, n, f->E, fscale);
     if (rc) return rc;
@@ -669,29 +701,37 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
     // X[tau] for tau = 2..7 hold P^T(...) without R: add R_tau (X[1] already has it)
     for (int t = 2; t < 8; ++t)
       k_lincomb<<<g, kVT, 0, st>>>(f->X + t * N, 9 * N, one, f->X + t * N, 9 * N, one, f->E + t * N, 8 * N, d_ids, N);
+      note_launch();
   }
   for (int o = 0; o < n; ++o) mv[o]++;
   // periodicity: forward ||X8 - X0|| / (||X0|| + 1e-30); adjoint: ||P0^T lam1 + R0 - lam0|| / ...
   if (!trans) {
     Scal mone{nullptr, 0, 0, -1.0};
     k_lincomb<<<g, kVT, 0, st>>>(c.Tv, c.vs, one, f->X + 8 * N, 9 * N, mone, f->X, 9 * N, d_ids, N);
+    note_launch();
   } else {
     // lam0_check = P_0^T lam_1 + R_0 computed in place into X[0], then X[0] = lam_0
     Scal mone{nullptr, 0, 0, -1.0};
     rc = chain_accurate(c, d_ids, n, f->E, fscale, 0, 1);
     if (rc) return rc;
     k_lincomb<<<g, kVT, 0, st>>>(c.Tv, c.vs, one, f->X, 9 * N, mone, c.Xv, c.vs, d_ids, N);
+    note_launch();
     k_lincomb<<<g, kVT, 0, st>>>(f->X, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
+    note_launch();
     k_lincomb<<<g, kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
+    note_launch();
   }
   rc = sqnorm(c, c.Tv, c.vs, d_ids, n, S_TMP);
   if (rc) return rc;
   rc = sqnorm(c, f->X, 9 * N, d_ids, n, S_H0);
   if (rc) return rc;
   k_count_neg<<<dim3(kRedBlocks, n), kVT, 0, st>>>(c.partial, f->X, 9 * N, 9 * N, d_ids);
+  note_launch();
   k_reduce_partials<<<n, 32, 0, st>>>(f->scal, kScal, S_NEG, c.partial, 1, d_ids, 0);
+  note_launch();
   // outputs in cell order
   k_perm_scatter<<<g, kVT, 0, st>>>(out, 9 * N, f->X, 9 * N, 9, sy->d.perm, d_ids, N);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   rc = fetch_scal(c);
   if (rc) return rc;
@@ -749,15 +789,18 @@ int chain_apply_impl(orbit_factor_s* f, int n, int trans, int tau0, int tau1, co
   const dim3 g = vgrid(N, n);
   const int in = trans ? tau1 : tau0, out = trans ? tau0 : tau1;
   k_perm_gather<<<g, kVT, 0, st>>>(f->X + (int64_t)in * N, 9 * N, x_in, N, 1, sy->d.perm, d_ids, N);
+  note_launch();
   const double* E = nullptr;
   if (forcing) {
     k_perm_gather<<<g, kVT, 0, st>>>(f->E, 8 * N, forcing, 8 * N, 8, sy->d.perm, d_ids, N);
+    note_launch();
     E = f->E;
   }
   ORBIT_CUDA_TRY(cudaGetLastError());
   rc = chain_accurate(c, d_ids, n, E, fscale, tau0, tau1);
   if (rc) return rc;
   k_perm_scatter<<<g, kVT, 0, st>>>(x_out, N, f->X + (int64_t)out * N, 9 * N, 1, sy->d.perm, d_ids, N);
+  note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return fetch_scal(c);
 }

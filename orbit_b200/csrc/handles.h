@@ -73,6 +73,10 @@ struct orbit_factor_s {
   double* scal = nullptr;   // per orbit scalars
   double* h_scal = nullptr; // pinned mirror
   int persist_grid = 0;
+  // optional per-launch timing of the chain kernel and of factorizations
+  bool prof_on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_chain, prof_factor;
+  double prof_chain_bytes = 0.0, prof_factor_flops = 0.0;
   std::mutex mu;
   std::vector<void*> allocs;
 };

@@ -307,11 +307,24 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   }
   int grid = sms * occ;
   if (grid > D.total) grid = D.total;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (f->prof_on) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+  }
   k_chain<T><<<grid, kSolveThreads, smem, st>>>(D);
+  note_launch();
+  if (f->prof_on) {
+    cudaEventRecord(e1, st);
+    f->prof_chain.push_back({e0, e1});
+    f->prof_chain_bytes += (double)B * (tau1 - tau0) * S.fac_nnz * sizeof(T);
+  }
   ORBIT_CUDA_TRY(cudaGetLastError());
   if (trans && E) {
     dim3 g((unsigned)((S.N + 255) / 256), B);
     k_add_forcing<<<g, 256, 0, st>>>(X, E, d_orbit_ids, S.N, tau0, escale);
+    note_launch();
     ORBIT_CUDA_TRY(cudaGetLastError());
   }
   return ORBIT_OK;

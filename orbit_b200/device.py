@@ -193,6 +193,15 @@ class FactorBatch:
             _lib.check(rc)
         return out, info
 
+    def profile(self, mode: int):
+        """1: enable+reset, 0: disable+reset, 2: read -> dict of chain/factor timings."""
+        out = (C.c_double * 6)()
+        _lib.check(_lib.lib().orbit_factor_profile(self._h, int(mode), out))
+        if mode != 2:
+            return None
+        return {"chain_launches": int(out[0]), "chain_ms": out[1], "chain_bytes": out[2],
+                "factor_calls": int(out[3]), "factor_ms": out[4], "factor_flops": out[5]}
+
     def bytes(self):
         a, b = C.c_int64(), C.c_int64()
         _lib.check(_lib.lib().orbit_factor_bytes(self._h, C.byref(a), C.byref(b)))
@@ -208,6 +217,11 @@ class FactorBatch:
             self.close()
         except Exception:
             pass
+
+
+def kernel_launches() -> int:
+    """Kernels liborbit_b200 has launched so far (process-wide)."""
+    return int(_lib.lib().orbit_kernel_launches())
 
 
 INFO_FIELDS = ("gmres_iters", "residual", "periodicity", "neg_frac", "converged", "s_norm",
