@@ -297,8 +297,103 @@ __global__ void k_update(FactorDev D, T* fronts, int64_t i0, int p0) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       int r = ty + 16 * i, c = tx + 16 * j;
-      if (r < h && c < w) F[(int64_t)(r0 + r) * ldf + c0 + c] -= acc[i][j];
+      if (r < h && c < w && (r0 + r < n || c0 + c < n)) F[(int64_t)(r0 + r) * ldf + c0 + c] -= acc[i][j];
     }
+}
+
+// Schur complement of a front: F22 -= L21 U12 (K = n), one 128 x 128 output
+// tile per CTA.  Register-tiled outer products (TM x TN per thread) from
+// shared-memory stages, with the next K slab prefetched into registers while
+// the current one is multiplied.
+template <typename T, int TM, int TN, int BN>
+__device__ __forceinline__ void schur_tile(const T* __restrict__ A, const T* __restrict__ B, T* C,
+                                           int ld, int K, int h, int w, T* As, T* Bs) {
+  constexpr int BM = 128, BK = 16;
+  constexpr int LDA = BM + 4, LDB = BN + 4;
+  constexpr int AL = BM * BK / 256, BL = BK * BN / 256;
+  const int tid = threadIdx.x, tx = tid % (BN / TN), ty = tid / (BN / TN);
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+  T ra[AL], rb[BL];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < AL; ++q) {
+      const int e = tid + q * 256, r = e / BK, kk = e % BK;
+      ra[q] = (r < h && k0 + kk < K) ? A[(int64_t)r * ld + k0 + kk] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < BL; ++q) {
+      const int e = tid + q * 256, kk = e / BN, c = e % BN;
+      rb[q] = (c < w && k0 + kk < K) ? B[(int64_t)(k0 + kk) * ld + c] : T(0);
+    }
+  };
+  load(0);
+  for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+    for (int q = 0; q < AL; ++q) {
+      const int e = tid + q * 256;
+      As[(e % BK) * LDA + e / BK] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < BL; ++q) {
+      const int e = tid + q * 256;
+      Bs[(e / BN) * LDB + e % BN] = rb[q];
+    }
+    __syncthreads();
+    if (k0 + BK < K) load(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      T a[TM], b[TN];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) a[i] = As[kk * LDA + ty * TM + i];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) b[j] = Bs[kk * LDB + tx * TN + j];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int r = ty * TM + i;
+    if (r >= h) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int c = tx * TN + j;
+      if (c < w) C[(int64_t)r * ld + c] -= acc[i][j];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_schur(FactorDev D, T* fronts, int64_t i0) {
+  extern __shared__ unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, tr = it.y, tc = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  const int r0 = 128 * tr, c0 = 128 * tc;
+  const int h = min(128, m - r0);
+  const T* A = F + (int64_t)(n + r0) * ldf;
+  if constexpr (sizeof(T) == 4) {
+    T* Bs = As + 16 * (128 + 4);
+    schur_tile<T, 8, 8, 128>(A, F + n + c0, F + (int64_t)(n + r0) * ldf + n + c0, ldf, n, h,
+                             min(128, m - c0), As, Bs);
+  } else {
+    T* Bs = As + 16 * (128 + 4);
+    for (int half = 0; half < 2; ++half) {
+      const int cc = c0 + 64 * half;
+      if (cc >= m) break;
+      schur_tile<T, 8, 4, 64>(A, F + n + cc, F + (int64_t)(n + r0) * ldf + n + cc, ldf, n, h,
+                              min(64, m - cc), As, Bs);
+    }
+  }
 }
 
 template <typename T>
@@ -439,6 +534,8 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   const size_t sm_gemm = 2 * 16 * kLdS * sizeof(T);
   const size_t sm_inv = sm_gemm + 64 * kLdS * sizeof(T);
   const size_t sm_diag = 3 * 64 * kLdS * sizeof(T);
+  const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
+  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_schur));
   ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_diag));
   ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_inv));
   {
@@ -488,6 +585,12 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
         case FactorLaunch::UPDATE: {
           dim3 g((unsigned)L.items, G);
           k_update<T><<<g, kThreads, sm_gemm, st>>>(D, cur, L.item_off, L.p0);
+          note_launch();
+          break;
+        }
+        case FactorLaunch::SCHUR: {
+          dim3 g((unsigned)L.items, G);
+          k_schur<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off);
           note_launch();
           break;
         }

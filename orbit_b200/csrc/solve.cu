@@ -81,6 +81,138 @@ __device__ __forceinline__ T dot_row(const T* __restrict__ a, const T* v, int le
   return warp_sum((acc0 + acc1) + (acc2 + acc3));
 }
 
+// Forward step of one supernode (L, or U^T when trans) for output rows
+// [r0, r1): gathers its right-hand side (own entries of Xin, plus forcing) and
+// the children's update vectors into `vec`, then one dense GEMV.  Ends with a
+// block barrier.
+template <typename T>
+__device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
+                         T* vec, T* red) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t N = D.N;
+  const int n = D.n[s], m = D.m[s], first = D.first[s];
+  const int ldn = D.ldn[s], ldm = D.ldm[s];
+  const T* SQ = D.factors + (int64_t)(o * 8 + tau) * D.fac_size + D.fac_off[s];
+  double* Yo = D.Y + (int64_t)o * N;
+  double* Wo = D.W + (int64_t)o * D.w_size;
+  const int bin_in = trans ? tau + 1 : tau;
+  const double* Xin = D.X + ((int64_t)o * 9 + bin_in) * N;
+  const double* Ein = nullptr;
+  if (D.E) {
+    if (!trans) Ein = D.E + ((int64_t)o * 8 + tau) * N;
+    else if (tau + 1 < D.tau1) Ein = D.E + ((int64_t)o * 8 + tau + 1) * N;
+  }
+  for (int i = tid; i < n + m; i += kSolveThreads) {
+    double v = 0.0;
+    if (i < n) {
+      v = Xin[first + i];
+      if (Ein) v += D.escale * Ein[first + i];
+    }
+    vec[i] = (T)v;
+  }
+  for (int q2 = 0; q2 < 2; ++q2) {
+    __syncthreads();
+    const int c = D.child[2 * s + q2];
+    if (c < 0) continue;
+    const int mc = D.m[c];
+    const int32_t* rel = D.rel + D.uoff[c];
+    const double* wc = Wo + D.woff[c];
+    for (int j = tid; j < mc; j += kSolveThreads) vec[rel[j]] += (T)wc[j];
+  }
+  __syncthreads();
+  if (!trans) {
+    // rows of [SQ; Pb]: row i < n uses the strict lower part (unit diagonal)
+    for (int i = r0 + warp; i < r1; i += kWarps) {
+      const int len = i < n ? i : n;
+      T acc = dot_row(SQ + (int64_t)i * ldn, vec, len, lane);
+      if (lane == 0) {
+        if (i < n) Yo[first + i] = (double)(vec[i] + acc);
+        else Wo[D.woff[s] + (i - n)] = (double)(vec[i] + acc);
+      }
+    }
+  } else {
+    // columns of [upper(SQ) | Qr]
+    const T* Qr = SQ + (int64_t)(n + m) * ldn;
+    for (int cb = r0; cb < r1; cb += 32) {
+      const int c = cb + lane;
+      T acc = T(0);
+      if (c < r1) {
+        if (c < n) {
+          for (int i = warp; i <= c; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
+        } else {
+          const int u = c - n;
+          for (int i = warp; i < n; i += kWarps) acc = fma(__ldg(Qr + (int64_t)i * ldm + u), vec[i], acc);
+        }
+      }
+      red[warp * 32 + lane] = acc;
+      __syncthreads();
+      if (warp == 0 && c < r1) {
+        T sum = T(0);
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) sum += red[w * 32 + lane];
+        if (c < n) Yo[first + c] = (double)sum;
+        else Wo[D.woff[s] + (c - n)] = (double)(vec[c] + sum);
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+}
+
+// Backward step of one supernode (U, or L^T when trans) for rows [r0, r1):
+// own forward result plus the ancestors' solution.  Ends with a block barrier.
+template <typename T>
+__device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
+                         T* vec, T* red) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t N = D.N;
+  const int n = D.n[s], m = D.m[s], first = D.first[s];
+  const int ldn = D.ldn[s], ldm = D.ldm[s];
+  const T* SQ = D.factors + (int64_t)(o * 8 + tau) * D.fac_size + D.fac_off[s];
+  const double* Yo = D.Y + (int64_t)o * N;
+  const int bin_out = trans ? tau : tau + 1;
+  double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
+  const int32_t* ui = D.uidx + D.uoff[s];
+  for (int i = tid; i < n + m; i += kSolveThreads) vec[i] = (T)(i < n ? Yo[first + i] : Xout[ui[i - n]]);
+  __syncthreads();
+  if (!trans) {
+    const T* Qr = SQ + (int64_t)(n + m) * ldn;
+    for (int i = r0 + warp; i < r1; i += kWarps) {
+      const T* row = SQ + (int64_t)i * ldn;
+      T acc0 = T(0), acc1 = T(0);
+      for (int j = i + lane; j < n; j += 32) acc0 = fma(__ldg(row + j), vec[j], acc0);
+      const T* qrow = Qr + (int64_t)i * ldm;
+      int j = lane;
+      for (; j + 32 < m; j += 64) {
+        acc1 = fma(__ldg(qrow + j), vec[n + j], acc1);
+        acc0 = fma(__ldg(qrow + j + 32), vec[n + j + 32], acc0);
+      }
+      for (; j < m; j += 32) acc1 = fma(__ldg(qrow + j), vec[n + j], acc1);
+      T acc = warp_sum(acc0 + acc1);
+      if (lane == 0) Xout[first + i] = (double)acc;
+    }
+  } else {
+    // columns of [SQ_strict_lower ; Pb] with unit diagonal
+    for (int cb = r0; cb < r1; cb += 32) {
+      const int c = cb + lane;
+      T acc = T(0);
+      if (c < r1) {
+        for (int i = c + 1 + warp; i < n + m; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
+      }
+      red[warp * 32 + lane] = acc;
+      __syncthreads();
+      if (warp == 0 && c < r1) {
+        T sum = vec[c];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) sum += red[w * 32 + lane];
+        Xout[first + c] = (double)sum;
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_chain(ChainDev<T> D) {
   extern __shared__ unsigned char smem_raw[];
@@ -88,9 +220,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_chain(ChainDev<T> D) {
   T* vec = red + kWarps * 32;                    // front-sized vector
   __shared__ int s_task;
   __shared__ int s_ok;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const int per_bin = D.items_per_bin * D.B;
-  const int64_t N = D.N;
   for (;;) {
     if (tid == 0) {
       s_task = atomicAdd(D.task_counter, 1);
@@ -109,26 +240,23 @@ __global__ void __launch_bounds__(kSolveThreads) k_chain(ChainDev<T> D) {
     const int oi = rr / cnt;
     const int4 it = D.items[D.phase_off[p] + (rr - oi * cnt)];
     const int o = D.orbit_ids[oi];
-    const int s = it.x, r0 = it.y, r1 = it.z, kind = it.w;
-    const int n = D.n[s], m = D.m[s], first = D.first[s];
-    const int ldn = D.ldn[s], ldm = D.ldm[s];
-    const T* SQ = D.factors + (int64_t)(o * 8 + tau) * D.fac_size + D.fac_off[s];
+    const int s = it.x, kind = it.w;
+    const bool fwd = (kind & 1) == 0;        // kinds 0, 2, 4, 6
+    const bool trans = kind == 2 || kind == 3 || kind == 6 || kind == 7;
+    const bool subtree = kind >= 4;
     int* cbase = D.counters + (int64_t)o * 8 * 2 * D.nsuper;
-    double* Yo = D.Y + (int64_t)o * N;
-    double* Wo = D.W + (int64_t)o * D.w_size;
     // ---- dependencies ----
     if (tid == 0) {
       bool ok = true;
-      if (kind == 0 || kind == 2) {
-        for (int q2 = 0; q2 < 2 && ok; ++q2) {
-          int c = D.child[2 * s + q2];
-          if (c >= 0)
-            ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, kind == 0 ? D.nch_f[c] : D.nch_f[c],
-                         D.status, D.spin_limit);
-        }
-        if (ok && kind == 0 && tau > D.tau0)
+      if (fwd) {
+        if (!subtree)
+          for (int q2 = 0; q2 < 2 && ok; ++q2) {
+            const int c = D.child[2 * s + q2];
+            if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
+          }
+        if (ok && !trans && tau > D.tau0)
           ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
-        if (ok && kind == 2 && tau < D.tau1 - 1)
+        if (ok && trans && tau < D.tau1 - 1)
           ok = wait_ge(cbase + ((tau + 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
       } else {
         const int par = D.parent[s];
@@ -142,119 +270,20 @@ __global__ void __launch_bounds__(kSolveThreads) k_chain(ChainDev<T> D) {
     }
     __syncthreads();
     if (!s_ok) break;
-    if (kind == 0 || kind == 2) {
-      // forward (L or U^T) step: gather own right-hand side and children's updates
-      const int bin_in = kind == 0 ? tau : tau + 1;
-      const double* Xin = D.X + ((int64_t)o * 9 + bin_in) * N;
-      const double* Ein = nullptr;
-      if (D.E) {
-        if (kind == 0) Ein = D.E + ((int64_t)o * 8 + tau) * N;
-        else if (tau + 1 < D.tau1) Ein = D.E + ((int64_t)o * 8 + tau + 1) * N;
-      }
-      for (int i = tid; i < n + m; i += kSolveThreads) {
-        double v = 0.0;
-        if (i < n) {
-          v = Xin[first + i];
-          if (Ein) v += D.escale * Ein[first + i];
-        }
-        vec[i] = (T)v;
-      }
-      for (int q2 = 0; q2 < 2; ++q2) {
-        __syncthreads();
-        const int c = D.child[2 * s + q2];
-        if (c < 0) continue;
-        const int mc = D.m[c];
-        const int32_t* rel = D.rel + D.uoff[c];
-        const double* wc = Wo + D.woff[c];
-        for (int j = tid; j < mc; j += kSolveThreads) vec[rel[j]] += (T)wc[j];
-      }
-      __syncthreads();
-      if (kind == 0) {
-        // rows of [SQ; Pb]: row i < n uses the strict lower part (unit diagonal)
-        for (int i = r0 + warp; i < r1; i += kWarps) {
-          const int len = i < n ? i : n;
-          T acc = dot_row(SQ + (int64_t)i * ldn, vec, len, lane);
-          if (lane == 0) {
-            if (i < n) Yo[first + i] = (double)(vec[i] + acc);
-            else Wo[D.woff[s] + (i - n)] = (double)(vec[i] + acc);
-          }
-        }
-      } else {
-        // columns of [upper(SQ) | Qr]
-        const T* Qr = SQ + (int64_t)(n + m) * ldn;
-        for (int cb = r0; cb < r1; cb += 32) {
-          const int c = cb + lane;
-          T acc = T(0);
-          if (c < r1) {
-            if (c < n) {
-              for (int i = warp; i <= c; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
-            } else {
-              const int u = c - n;
-              for (int i = warp; i < n; i += kWarps) acc = fma(__ldg(Qr + (int64_t)i * ldm + u), vec[i], acc);
-            }
-          }
-          red[warp * 32 + lane] = acc;
-          __syncthreads();
-          if (warp == 0 && c < r1) {
-            T sum = T(0);
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) sum += red[w * 32 + lane];
-            if (c < n) Yo[first + c] = (double)sum;
-            else Wo[D.woff[s] + (c - n)] = (double)(vec[c] + sum);
-          }
-          __syncthreads();
-        }
-      }
+    if (!subtree) {
+      if (fwd) fwd_node(D, o, tau, s, it.y, it.z, trans, vec, red);
+      else bwd_node(D, o, tau, s, it.y, it.z, trans, vec, red);
+    } else if (fwd) {
+      // postorder: every child before its parent
+      for (int d = it.y; d <= s; ++d)
+        fwd_node(D, o, tau, d, 0, trans ? D.n[d] + D.m[d] : D.n[d] + D.m[d], trans, vec, red);
     } else {
-      // backward (U or L^T) step: own forward result plus ancestors' solution
-      const int bin_out = kind == 1 ? tau + 1 : tau;
-      double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
-      const int32_t* ui = D.uidx + D.uoff[s];
-      for (int i = tid; i < n + m; i += kSolveThreads)
-        vec[i] = (T)(i < n ? Yo[first + i] : Xout[ui[i - n]]);
-      __syncthreads();
-      if (kind == 1) {
-        const T* Qr = SQ + (int64_t)(n + m) * ldn;
-        for (int i = r0 + warp; i < r1; i += kWarps) {
-          const T* row = SQ + (int64_t)i * ldn;
-          T acc0 = T(0), acc1 = T(0);
-          for (int j = i + lane; j < n; j += 32) acc0 = fma(__ldg(row + j), vec[j], acc0);
-          const T* qrow = Qr + (int64_t)i * ldm;
-          int j = lane;
-          for (; j + 32 < m; j += 64) {
-            acc1 = fma(__ldg(qrow + j), vec[n + j], acc1);
-            acc0 = fma(__ldg(qrow + j + 32), vec[n + j + 32], acc0);
-          }
-          for (; j < m; j += 32) acc1 = fma(__ldg(qrow + j), vec[n + j], acc1);
-          T acc = warp_sum(acc0 + acc1);
-          if (lane == 0) Xout[first + i] = (double)acc;
-        }
-      } else {
-        // columns of [SQ_strict_lower ; Pb] with unit diagonal
-        for (int cb = r0; cb < r1; cb += 32) {
-          const int c = cb + lane;
-          T acc = T(0);
-          if (c < r1) {
-            for (int i = c + 1 + warp; i < n + m; i += kWarps)
-              acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
-          }
-          red[warp * 32 + lane] = acc;
-          __syncthreads();
-          if (warp == 0 && c < r1) {
-            T sum = vec[c];
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) sum += red[w * 32 + lane];
-            Xout[first + c] = (double)sum;
-          }
-          __syncthreads();
-        }
-      }
+      // reverse postorder: every parent before its children
+      for (int d = s; d >= it.y; --d) bwd_node(D, o, tau, d, 0, D.n[d], trans, vec, red);
     }
-    __syncthreads();
     if (tid == 0) {
       __threadfence();
-      const int ph = (kind == 0 || kind == 2) ? 0 : 1;
-      red_release_add(cbase + (tau * 2 + ph) * D.nsuper + s, 1);
+      red_release_add(cbase + (tau * 2 + (fwd ? 0 : 1)) * D.nsuper + s, 1);
     }
   }
 }

@@ -304,10 +304,25 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
         int nb = std::min(kNB, S.n[s] - p0);
         int rest = S.n[s] + S.m[s] - (p0 + nb);
         int nt = (rest + kTile - 1) / kTile;
+        const int q0 = p0 + nb;
+        // only tiles touching the pivot rows or columns; the ancestor block
+        // F22 is updated once, after the last pivot block (SCHUR)
+        for (int tr = 0; tr < nt; ++tr)
+          for (int tc = 0; tc < nt; ++tc)
+            if (q0 + kTile * tr < S.n[s] || q0 + kTile * tc < S.n[s]) push_item(s, tr, tc, 0);
+      }
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::UPDATE, l, p0, off, nitems() - off});
+    }
+    {
+      int64_t off = nitems();
+      for (int s : sups) {
+        const int mm = S.m[s];
+        if (mm == 0 || S.n[s] == 0) continue;
+        const int nt = (mm + kSchurTile - 1) / kSchurTile;
         for (int tr = 0; tr < nt; ++tr)
           for (int tc = 0; tc < nt; ++tc) push_item(s, tr, tc, 0);
       }
-      if (nitems() > off) S.fsched.push_back({FactorLaunch::UPDATE, l, p0, off, nitems() - off});
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::SCHUR, l, 0, off, nitems() - off});
     }
     // blocked triangular inverses: step t fills block row t of Linv and block column t of Uinv
     int tmax = (nmax + kNB - 1) / kNB;
@@ -356,12 +371,47 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     }
     return cnt;
   };
+  // Subtree tasks: below a work threshold a whole subtree is one task (its
+  // nodes are a contiguous postorder range), which removes the per-level
+  // dependency waits of the many small supernodes near the leaves.
+  std::vector<int64_t> subw(ns, 0);
+  std::vector<int32_t> sub_node_first(ns);
+  for (int s = 0; s < ns; ++s) {
+    int64_t w = int64_t(S.n[s]) * S.n[s] + 2 * int64_t(S.n[s]) * S.m[s];
+    int32_t f = s;
+    for (int q = 0; q < 2; ++q) {
+      int c = S.child[2 * s + q];
+      if (c >= 0) {
+        w += subw[c];
+        f = std::min(f, sub_node_first[c]);
+      }
+    }
+    subw[s] = w;
+    sub_node_first[s] = f;
+  }
+  const int64_t wmax = std::max<int64_t>(int64_t(4) * chunk_elems, S.fac_nnz / 256);
+  // role: 0 = chunked node, 1 = subtree root, 2 = inside a subtree
+  S.role.assign(ns, 0);
+  for (int s = ns - 1; s >= 0; --s) {
+    const int p = S.parent[s];
+    if (p >= 0 && S.role[p] != 0) S.role[s] = 2;
+    else if (subw[s] <= wmax && (S.nchild[s] > 0 || p < 0 || subw[p] > wmax)) S.role[s] = 1;
+  }
+  auto push4 = [&](int a, int b, int c, int d) {
+    S.sitems.push_back(a); S.sitems.push_back(b); S.sitems.push_back(c); S.sitems.push_back(d);
+  };
   // non-transposed: fwd levels deep->0, bwd levels 0->deep
   S.phase_off.clear();
   for (int l = S.nlevels - 1; l >= 0; --l) {
     S.phase_off.push_back(int32_t(S.sitems.size() / 4));
     for (int s : S.level_sups[l]) {
       int n = S.n[s], m = S.m[s];
+      if (S.role[s] == 2) continue;
+      if (S.role[s] == 1) {
+        push4(s, sub_node_first[s], 0, 4);
+        S.nchunk_fwd[s] = 1;
+        continue;
+      }
       S.nchunk_fwd[s] = chunk_rows(s, 0, n + m, [n](int r) { return r < n ? int64_t(r) : int64_t(n); });
     }
   }
@@ -369,6 +419,12 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     S.phase_off.push_back(int32_t(S.sitems.size() / 4));
     for (int s : S.level_sups[l]) {
       int n = S.n[s], m = S.m[s];
+      if (S.role[s] == 2) continue;
+      if (S.role[s] == 1) {
+        push4(s, sub_node_first[s], 0, 5);
+        S.nchunk_bwd[s] = 1;
+        continue;
+      }
       S.nchunk_bwd[s] = chunk_rows(s, 1, n, [n, m](int r) { return int64_t(n - r + m); });
     }
   }
@@ -381,6 +437,12 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
     for (int s : S.level_sups[l]) {
       int n = S.n[s], m = S.m[s];
+      if (S.role[s] == 2) continue;
+      if (S.role[s] == 1) {
+        push4(s, sub_node_first[s], 0, 6);
+        S.nchunk_fwdT[s] = 1;
+        continue;
+      }
       S.nchunk_fwdT[s] = chunk_rows(s, 2, n + m, [n](int c) { return c < n ? int64_t(c + 1) : int64_t(n); });
     }
   }
@@ -388,6 +450,12 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
     for (int s : S.level_sups[l]) {
       int n = S.n[s], m = S.m[s];
+      if (S.role[s] == 2) continue;
+      if (S.role[s] == 1) {
+        push4(s, sub_node_first[s], 0, 7);
+        S.nchunk_bwdT[s] = 1;
+        continue;
+      }
       S.nchunk_bwdT[s] = chunk_rows(s, 3, n, [n, m](int c) { return int64_t(n - c + m); });
     }
   }

@@ -23,12 +23,13 @@ enum StencilDir { D_C = 0, D_W = 1, D_E = 2, D_S = 3, D_N = 4, D_B = 5, D_T = 6 
 constexpr int kTile = 64;      // dense tile edge of the factorization kernels
 constexpr int kNB = 64;        // panel width of the blocked LU
 constexpr int kPad = 4;        // leading-dimension padding (elements)
+constexpr int kSchurTile = 128;  // output tile edge of the Schur-complement GEMM
 
 inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 // One kernel launch of the numeric factorization schedule.
 struct FactorLaunch {
-  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, INV, PROD } kind;
+  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, PROD } kind;
   int level;
   int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV)
   int64_t item_off;  // offset into the item array (int4 units)
@@ -70,13 +71,15 @@ struct Symbolic {
   std::vector<int32_t> fitems;            // 4 ints per item
   std::vector<FactorLaunch> fsched;
   // solve schedule (per bin, shared by all instances): items {s, r0, r1, kind}
-  // kinds: 0 fwd, 1 bwd, 2 fwdT, 3 bwdT
+  // kinds: 0 fwd, 1 bwd, 2 fwdT, 3 bwdT (row chunks of one supernode);
+  // 4..7 the same sweeps over a whole subtree {root, first node, 0, kind}
   std::vector<int32_t> sitems;            // 4 ints per item
   std::vector<int32_t> phase_off;         // non-transposed phases (2*nlevels+1 offsets)
   std::vector<int32_t> phase_offT;        // transposed phases
   int32_t items_per_bin = 0, items_per_binT = 0;
   // per supernode number of chunks in each solve kind
   std::vector<int32_t> nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT;
+  std::vector<int32_t> role;  // 0 chunked node, 1 subtree-task root, 2 inside a subtree
   int max_front = 0;
   int max_nm = 0;
   double factor_flops = 0.0;
