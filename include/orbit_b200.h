@@ -131,6 +131,21 @@ int orbit_mass_balance_rows(int nz, int ny, int nx, int nbins, const double* con
 int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
                      const double* c, double dt, int limited, double* d, orbit_stream_t stream);
 
+/* K2 without device allocation, for callers that cannot allocate device
+ * memory at the point where they apply the FCT correction (a host model that
+ * owns its whole device-memory budget through its own pool, or a time loop
+ * that must not stall on the synchronization cudaFree can cause).  Same inputs,
+ * outputs and results as orbit_fct_source.  No counterpart in the reference.
+ * The scratch (x = c/rho, R+, R-) is one static device array of 3 x 2^20
+ * doubles (24 MiB) that every GPU loading this library holds until exit, so
+ * n_vec*nz*ny*nx must be <= 1,048,576 (larger requests return ORBIT_ERR_ARG).
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array, so calls
+ * that overlap on the GPU (different streams or threads) race: serialize them. */
+int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
+                             const double* c, double dt, int limited, double* d,
+                             orbit_stream_t stream);
+
 /* A batch of n_orbits x 8 numeric factorizations of A = I + dtau (T + diag(sink))
  * sharing one symbolic.  precision = ORBIT_PREC_FP64 or ORBIT_PREC_FP32.
  * Replaces _factor_one_bin / _UmfpackLU.__init__ (orbit/core/orbit.py:79-96,

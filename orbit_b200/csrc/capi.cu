@@ -32,6 +32,8 @@ int mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* Ts
                       const double* const* rho, double* out_int, double* out_top, cudaStream_t st);
 int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
                int limited, double* d, double* scratch, cudaStream_t st);
+int fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
+                       double dt, int limited, double* d, cudaStream_t st);
 
 namespace {
 
@@ -318,6 +320,15 @@ int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, 
   int rc = fct_source(nz, ny, nx, met, n_vec, c, dt, limited, d, scratch, st);
   cudaFreeAsync(scratch, st);
   return rc;
+}
+
+int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
+                             double dt, int limited, double* d, orbit_stream_t stream) {
+  if (!met || !c || !d || n_vec < 1 || nz < 1 || ny < 1 || nx < 1 || !(dt > 0)) {
+    set_last_error("orbit_fct_source_noalloc: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  return fct_source_noalloc(nz, ny, nx, met, n_vec, c, dt, limited, d, (cudaStream_t)stream);
 }
 
 int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit_factor_t* out) {

@@ -222,3 +222,64 @@ int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const 
 }
 
 }  // namespace orbit
+
+// ---------------------------------------------------------------------------
+// FCT source without any device allocation.
+//
+// Some callers cannot allocate device memory when they apply the correction:
+// a host model that hands this library a fixed device-memory budget and owns
+// every other byte through its own pool, or a time-stepping loop that must not
+// stall on the implicit synchronization cudaFree may cause.  For them the
+// three per-cell scratch arrays of the two FCT passes (x = c / rho and the
+// Zalesak ratios R+ and R-) live in one file-scope device array instead of a
+// stream-ordered allocation.  Every GPU that loads the library holds the
+// array (kFctNoAllocMaxCells doubles x 3, 24 MiB) until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace orbit {
+
+// n_vec * nz * ny * nx may not exceed this (e.g. 12 vectors of 86,400 cells).
+constexpr int64_t kFctNoAllocMaxCells = int64_t(1) << 20;
+
+static __device__ __align__(256) double g_fct_scratch[3 * kFctNoAllocMaxCells];
+
+namespace {
+std::mutex g_fct_scratch_mu;
+constexpr int kMaxDevices = 64;
+double* g_fct_scratch_ptr[kMaxDevices] = {nullptr};
+}  // namespace
+
+int fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
+                       double dt, int limited, double* d, cudaStream_t st) {
+  const int64_t cells = (int64_t)nz * ny * nx * n_vec;
+  if (cells > kFctNoAllocMaxCells) {
+    set_last_error("orbit_fct_source_noalloc: n_vec*nz*ny*nx = " + std::to_string(cells) +
+                   " exceeds the static scratch limit of " + std::to_string(kFctNoAllocMaxCells) +
+                   " cells; split the vectors over several calls or use orbit_fct_source");
+    return ORBIT_ERR_ARG;
+  }
+  int dev = 0;
+  ORBIT_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_last_error("orbit_fct_source_noalloc: device ordinal out of range");
+    return ORBIT_ERR_ARG;
+  }
+  double* scratch = nullptr;
+  {
+    // The array's name is only a host-side stand-in for the symbol; its device
+    // address is looked up once per device, with that device current.
+    std::lock_guard<std::mutex> lk(g_fct_scratch_mu);
+    if (!g_fct_scratch_ptr[dev]) {
+      void* p = nullptr;
+      ORBIT_CUDA_TRY(cudaGetSymbolAddress(&p, g_fct_scratch));
+      g_fct_scratch_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_fct_scratch_ptr[dev];
+  }
+  // x, R+ and R- are fully overwritten by the passes that produce them, so the
+  // scratch needs no clearing between calls.
+  return fct_source(nz, ny, nx, met, n_vec, c, dt, limited, d, scratch, st);
+}
+
+}  // namespace orbit
