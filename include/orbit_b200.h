@@ -87,9 +87,10 @@ typedef struct {
 int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out);
 /* Replaces umfpack_free_symbolic (orbit/core/solve.py:291-296). */
 int orbit_symbolic_destroy(orbit_symbolic_t sym);
-/* info[0..11] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor
+/* info[0..12] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor
  * elements per instance, front elements per instance, max front, factor
- * flops, solve items per bin, update-vector length, leaf_cells, max n/m. */
+ * flops, solve items per bin, update-vector length, leaf_cells, max n/m,
+ * largest front inside a subtree solve task. */
 int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info);
 /* perm[new] = cell (host array of N int32). */
 int orbit_symbolic_perm(orbit_symbolic_t sym, int32_t* perm_host);
@@ -151,9 +152,20 @@ int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int
  * Replaces _factor_one_bin / _UmfpackLU.__init__ (orbit/core/orbit.py:79-96,
  * orbit/core/solve.py:210-243). */
 int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit_factor_t* out);
+/* General form: n_orbits solve slots over n_sets factor sets of n_bins (8)
+ * factorizations each; slot o uses set (o % n_sets) until orbit_factor_map
+ * says otherwise, so many right-hand sides can share one operator (the
+ * reference reuses one lu_list_8 for all marginal and adjoint right-hand
+ * sides, orbit/modes/adjoint.py:573-583).  n_bins = 1 (with one slot and one
+ * set) holds a single factorization: the per-bin LU object the reference's
+ * _factor_one_bin returns (orbit/core/orbit.py:79-96). */
+int orbit_factor_create_ex(orbit_symbolic_t sym, int n_orbits, int n_sets, int n_bins, int precision,
+                           orbit_factor_t* out);
+/* Factor set used by each solve slot (host array of n_orbits indices). */
+int orbit_factor_map(orbit_factor_t f, const int32_t* set_of_orbit);
 int orbit_factor_destroy(orbit_factor_t f);
-/* Factor all (or the first n_active) orbits.  T_stencils / sink_diags are host
- * arrays of n_active*8 device pointers (orbit-major, bin-minor); a sink
+/* Factor the first n_active factor sets.  T_stencils / sink_diags are host
+ * arrays of n_active*n_bins device pointers (set-major, bin-minor); a sink
  * pointer may be NULL.  The stencils are copied; callers may free them after
  * the call returns (stream-ordered). */
 int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_stencils,

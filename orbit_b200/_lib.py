@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liborbit_b200.so")
+LIB_PATH = os.environ.get("ORBIT_B200_LIB") or os.path.join(HERE, "liborbit_b200.so")
 
 ORBIT_OK = 0
 ERR_NAMES = {1: "ORBIT_ERR_ARG", 2: "ORBIT_ERR_NOMEM", 3: "ORBIT_ERR_CUDA", 4: "ORBIT_ERR_TIMEOUT",
@@ -57,6 +57,9 @@ EXPORTS = {
     "orbit_fct_source_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_int,
                                            C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_factor_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "orbit_factor_create_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_void_p)]),
+    "orbit_factor_map": (C.c_int, [C.c_void_p, C.c_void_p]),
     "orbit_factor_destroy": (C.c_int, [C.c_void_p]),
     "orbit_factor_numeric": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
                                        C.c_void_p]),

@@ -71,3 +71,37 @@ class OrbitSolver:
         out[:n] = orb.cpu().numpy()
         self.d2h_bytes += n * (N_BINS + 1) * self.N * 8
         return out, [device.info_dict(r) for r in info]
+
+
+def solve_with_fct(fb: "device.FactorBatch", mets: Sequence["device.MetDevice"], E: torch.Tensor,
+                   passes: int, tol: float, maxiter: int = 200, dtau: float = DTAU):
+    """Deferred FCT correction on already factored orbits (the forward driver's
+    schedule, orbit/cli.py:1204-1241): pass 0 without FCT, then ``passes``
+    solves whose right-hand side adds the limited anti-diffusive source of the
+    previous pass's end-of-bin concentrations, warm-started from the previous
+    c_0.  All orbits of the batch and all bins run on the device (K2 per bin
+    over every orbit at once).  Returns the final orbits and a list of the
+    per-pass info arrays."""
+    orb, info = fb.solve(E, tol=tol, maxiter=maxiter, dtau=dtau)
+    infos = [info]
+    n = E.shape[0]
+    for _ in range(passes):
+        d = torch.stack([device.fct_source(mets[t], orb[:, t + 1].contiguous(), dtau) for t in range(N_BINS)],
+                        dim=1)  # (n, 8, N)
+        orb, info = fb.solve(E + d, c_warm=orb[:, 0].contiguous(), tol=tol, maxiter=maxiter, dtau=dtau)
+        infos.append(info)
+    return orb, infos
+
+
+def solve_shared_operator(sym: Symbolic, T_stencils: Sequence[torch.Tensor], sinks: Sequence[torch.Tensor],
+                          forcing: torch.Tensor, adjoint: bool = False, precision: int = 32,
+                          tol: float = 1e-6, maxiter: int = 200, dtau: float = DTAU):
+    """Many right-hand sides on one operator (marginal emission perturbations, or
+    adjoint receptors with the transposed chain): one factor set of 8 bins,
+    every solve slot mapped onto it, all orbits in one batched GMRES."""
+    n = forcing.shape[0]
+    fb = device.FactorBatch(sym, n, precision, n_sets=1)
+    fb.numeric(list(T_stencils), list(sinks), dtau)
+    if adjoint:
+        return fb.solve_adjoint(forcing, tol=tol, maxiter=maxiter)
+    return fb.solve(forcing, tol=tol, maxiter=maxiter, dtau=dtau)

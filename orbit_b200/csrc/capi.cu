@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -109,10 +110,11 @@ int build_device_symbolic(orbit_symbolic_s* h) {
   ORBIT_TRY(upload(A, &d.nchunk_bwdT, S.nchunk_bwdT));
   ORBIT_TRY(upload(A, &d.perm, S.perm));
   ORBIT_TRY(upload(A, &d.iperm, S.iperm));
+  ORBIT_TRY(upload(A, &d.level, S.level));
   return ORBIT_OK;
 }
 
-constexpr int kDefaultLeaf = 16;
+constexpr int kDefaultLeaf = 64;
 constexpr int kChunkElems = 8192;
 
 }  // namespace
@@ -184,7 +186,12 @@ int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic
   *out = nullptr;
   orbit_symbolic_s* h = new (std::nothrow) orbit_symbolic_s();
   if (!h) return ORBIT_ERR_NOMEM;
-  std::string err = build_symbolic(nz, ny, nx, leaf_cells > 0 ? leaf_cells : kDefaultLeaf, kChunkElems, h->S);
+  int chunk = kChunkElems;
+  if (const char* e = std::getenv("ORBIT_B200_CHUNK")) chunk = std::max(256, std::atoi(e));
+  int leaf = leaf_cells > 0 ? leaf_cells : kDefaultLeaf;
+  if (leaf_cells <= 0)
+    if (const char* e = std::getenv("ORBIT_B200_LEAF")) leaf = std::max(1, std::atoi(e));
+  std::string err = build_symbolic(nz, ny, nx, leaf, chunk, h->S);
   if (!err.empty()) {
     set_last_error(err);
     delete h;
@@ -207,9 +214,10 @@ int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info) {
     return ORBIT_ERR_ARG;
   }
   const Symbolic& S = sym->S;
-  int64_t v[12] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
-                   (int64_t)S.factor_flops, S.items_per_bin, S.w_size, S.leaf_cells, S.max_nm};
-  for (int i = 0; i < n_info && i < 12; ++i) info[i] = v[i];
+  int64_t v[13] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
+                   (int64_t)S.factor_flops, S.items_per_bin, S.w_size, S.leaf_cells, S.max_nm,
+                   S.max_sub_front};
+  for (int i = 0; i < n_info && i < 13; ++i) info[i] = v[i];
   return ORBIT_OK;
 }
 
@@ -331,9 +339,12 @@ int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int
   return fct_source_noalloc(nz, ny, nx, met, n_vec, c, dt, limited, d, (cudaStream_t)stream);
 }
 
-int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit_factor_t* out) {
-  if (!sym || !out || n_orbits < 1 || (precision != ORBIT_PREC_FP64 && precision != ORBIT_PREC_FP32)) {
-    set_last_error("orbit_factor_create: bad arguments");
+int orbit_factor_create_ex(orbit_symbolic_t sym, int n_orbits, int n_sets, int n_bins, int precision,
+                           orbit_factor_t* out) {
+  if (!sym || !out || n_orbits < 1 || n_sets < 1 || (n_bins != 1 && n_bins != 8) ||
+      (n_bins == 1 && (n_orbits != 1 || n_sets != 1)) ||
+      (precision != ORBIT_PREC_FP64 && precision != ORBIT_PREC_FP32)) {
+    set_last_error("orbit_factor_create_ex: bad arguments (n_bins is 8, or 1 with one orbit and one set)");
     return ORBIT_ERR_ARG;
   }
   *out = nullptr;
@@ -355,12 +366,14 @@ int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit
   if (!f) return ORBIT_ERR_NOMEM;
   f->sym = sym;
   f->n_orbits = n_orbits;
+  f->n_sets = n_sets;
+  f->n_bins = n_bins;
   f->precision = precision;
   cudaGetDevice(&f->device);
   const Symbolic& S = sym->S;
   const int64_t N = S.N;
   const size_t vb = precision == ORBIT_PREC_FP32 ? 4 : 8;
-  const int64_t n_inst = (int64_t)n_orbits * 8;
+  const int64_t n_inst = (int64_t)n_sets * n_bins;
   auto& A = f->allocs;
   int rc = ORBIT_OK;
   auto fail = [&](int code) {
@@ -384,8 +397,13 @@ int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit
   if ((rc = dalloc(A, &f->Wbuf, (size_t)n_orbits * S.w_size))) return fail(rc);
   if ((rc = dalloc(A, &f->counters, (size_t)n_orbits * 16 * S.nsuper))) return fail(rc);
   if ((rc = dalloc(A, &f->E, (size_t)n_orbits * 8 * N))) return fail(rc);
-  if ((rc = dalloc(A, &f->tmpv, (size_t)n_orbits * 15 * N))) return fail(rc);
+  if ((rc = dalloc(A, &f->tmpv, (size_t)n_orbits * 23 * N))) return fail(rc);
   if ((rc = dalloc(A, &f->orbit_ids, (size_t)n_orbits))) return fail(rc);
+  if ((rc = dalloc(A, &f->set_of, (size_t)n_orbits))) return fail(rc);
+  f->h_set_of.resize(n_orbits);
+  for (int o = 0; o < n_orbits; ++o) f->h_set_of[o] = o % n_sets;
+  if (cudaMemcpy(f->set_of, f->h_set_of.data(), sizeof(int) * n_orbits, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(ORBIT_ERR_CUDA);
   if ((rc = dalloc(A, &f->task_counter, (size_t)1 + n_orbits))) return fail(rc);
   if ((rc = dalloc(A, &f->status, (size_t)1))) return fail(rc);
   f->restart_cap = 31;
@@ -407,6 +425,26 @@ int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit
   return ORBIT_OK;
 }
 
+int orbit_factor_create(orbit_symbolic_t sym, int n_orbits, int precision, orbit_factor_t* out) {
+  return orbit_factor_create_ex(sym, n_orbits, n_orbits, 8, precision, out);
+}
+
+int orbit_factor_map(orbit_factor_t f, const int32_t* set_of_orbit) {
+  if (!f || !set_of_orbit) {
+    set_last_error("orbit_factor_map: null argument");
+    return ORBIT_ERR_ARG;
+  }
+  for (int o = 0; o < f->n_orbits; ++o)
+    if (set_of_orbit[o] < 0 || set_of_orbit[o] >= f->n_sets) {
+      set_last_error("orbit_factor_map: factor set index out of range");
+      return ORBIT_ERR_ARG;
+    }
+  std::lock_guard<std::mutex> lk(f->mu);
+  f->h_set_of.assign(set_of_orbit, set_of_orbit + f->n_orbits);
+  ORBIT_CUDA_TRY(cudaMemcpy(f->set_of, f->h_set_of.data(), sizeof(int) * f->n_orbits, cudaMemcpyHostToDevice));
+  return ORBIT_OK;
+}
+
 int orbit_factor_destroy(orbit_factor_t f) {
   if (!f) return ORBIT_OK;
   cudaDeviceSynchronize();
@@ -420,22 +458,23 @@ int orbit_factor_destroy(orbit_factor_t f) {
 
 int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_stencils,
                          const double* const* sink_diags, double dtau, orbit_stream_t stream) {
-  if (!f || !T_stencils || n_active < 1 || n_active > f->n_orbits || !(dtau > 0)) {
-    set_last_error("orbit_factor_numeric: bad arguments");
+  if (!f || !T_stencils || n_active < 1 || n_active > f->n_sets || !(dtau > 0)) {
+    set_last_error("orbit_factor_numeric: bad arguments (n_active factor sets <= n_sets)");
     return ORBIT_ERR_ARG;
   }
-  for (int i = 0; i < n_active * 8; ++i)
+  const int nb = f->n_bins;
+  for (int i = 0; i < n_active * nb; ++i)
     if (!T_stencils[i]) {
       set_last_error("orbit_factor_numeric: NULL transport stencil");
       return ORBIT_ERR_ARG;
     }
   std::lock_guard<std::mutex> lk(f->mu);
   cudaStream_t st = (cudaStream_t)stream;
-  std::vector<const double*> dp(n_active * 8, nullptr);
+  std::vector<const double*> dp(n_active * nb, nullptr);
   if (sink_diags)
-    for (int i = 0; i < n_active * 8; ++i) dp[i] = sink_diags[i];
-  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Tptr, T_stencils, sizeof(double*) * n_active * 8, cudaMemcpyHostToDevice, st));
-  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Dptr, dp.data(), sizeof(double*) * n_active * 8, cudaMemcpyHostToDevice, st));
+    for (int i = 0; i < n_active * nb; ++i) dp[i] = sink_diags[i];
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Tptr, T_stencils, sizeof(double*) * n_active * nb, cudaMemcpyHostToDevice, st));
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->d_Dptr, dp.data(), sizeof(double*) * n_active * nb, cudaMemcpyHostToDevice, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(int), st));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (f->prof_on) {
@@ -447,7 +486,7 @@ int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_
   if (f->prof_on) {
     cudaEventRecord(e1, st);
     f->prof_factor.push_back({e0, e1});
-    f->prof_factor_flops += (double)n_active * 8 * f->sym->S.factor_flops;
+    f->prof_factor_flops += (double)n_active * nb * f->sym->S.factor_flops;
   }
   if (rc) return rc;
   ORBIT_CUDA_TRY(cudaMemcpyAsync(f->h_status, f->status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -468,21 +507,39 @@ int orbit_factor_bytes(orbit_factor_t f, int64_t* numeric_bytes, int64_t* worksp
   }
   const Symbolic& S = f->sym->S;
   const int64_t vb = f->precision == ORBIT_PREC_FP32 ? 4 : 8;
-  if (numeric_bytes) *numeric_bytes = (int64_t)f->n_orbits * 8 * S.fac_size * vb;
+  if (numeric_bytes) *numeric_bytes = (int64_t)f->n_sets * f->n_bins * S.fac_size * vb;
   if (workspace_bytes)
     *workspace_bytes = (int64_t)2 * f->front_group * S.front_buf_size * vb +
-                       (int64_t)f->n_orbits * (7 * 8 + 9 + 1 + 8 + 15 + 33) * S.N * 8;
+                       (int64_t)f->n_sets * f->n_bins * 7 * S.N * 8 +
+                       (int64_t)f->n_orbits * (9 + 1 + 8 + 23 + 33) * S.N * 8;
+  return ORBIT_OK;
+}
+
+static int check_slots(orbit_factor_t f, int n_active, bool need_8_bins) {
+  if (need_8_bins && f->n_bins != 8) {
+    set_last_error("periodic-orbit solves need an 8-bin factor handle");
+    return ORBIT_ERR_ARG;
+  }
+  if (n_active < 1 || n_active > f->n_orbits) {
+    set_last_error("n_active out of range");
+    return ORBIT_ERR_ARG;
+  }
+  for (int o = 0; o < n_active; ++o)
+    if (f->h_set_of[o] >= f->n_factored) {
+      set_last_error("an active orbit maps to a factor set that has not been factored");
+      return ORBIT_ERR_ARG;
+    }
   return ORBIT_OK;
 }
 
 int orbit_chain_apply(orbit_factor_t f, int n_active, int trans, int tau0, int tau1, const double* x_in,
                       double* x_out, const double* forcing, double fscale, int refine,
                       orbit_stream_t stream) {
-  if (!f || !x_in || !x_out || n_active < 1 || n_active > f->n_factored || tau0 < 0 || tau1 > 8 ||
-      tau0 >= tau1) {
-    set_last_error("orbit_chain_apply: bad arguments (factor first; 0 <= tau0 < tau1 <= 8)");
+  if (!f || !x_in || !x_out || tau0 < 0 || tau1 > f->n_bins || tau0 >= tau1) {
+    set_last_error("orbit_chain_apply: bad arguments (0 <= tau0 < tau1 <= bins of the handle)");
     return ORBIT_ERR_ARG;
   }
+  if (int rc0 = check_slots(f, n_active, false)) return rc0;
   std::lock_guard<std::mutex> lk(f->mu);
   return chain_apply_impl(f, n_active, trans, tau0, tau1, x_in, x_out, forcing, fscale, refine,
                           (cudaStream_t)stream);
@@ -491,11 +548,11 @@ int orbit_chain_apply(orbit_factor_t f, int n_active, int trans, int tau0, int t
 int orbit_gmres_solve(orbit_factor_t f, int n_active, const double* e, double dtau, const double* c_warm,
                       double tol, int maxiter, int restart, double* orbit_out, double* info_out,
                       orbit_stream_t stream) {
-  if (!f || !e || !orbit_out || !info_out || n_active < 1 || n_active > f->n_factored || !(tol > 0) ||
-      maxiter < 1) {
+  if (!f || !e || !orbit_out || !info_out || !(tol > 0) || maxiter < 1) {
     set_last_error("orbit_gmres_solve: bad arguments");
     return ORBIT_ERR_ARG;
   }
+  if (int rc0 = check_slots(f, n_active, true)) return rc0;
   std::lock_guard<std::mutex> lk(f->mu);
   return orbit_solve_impl(f, n_active, e, dtau, c_warm, tol, maxiter, restart, orbit_out, info_out, 0,
                           (cudaStream_t)stream);
@@ -504,11 +561,11 @@ int orbit_gmres_solve(orbit_factor_t f, int n_active, const double* e, double dt
 int orbit_adjoint_gmres_solve(orbit_factor_t f, int n_active, const double* R, const double* lam_warm,
                               double tol, int maxiter, int restart, double* adjoint_out, double* info_out,
                               orbit_stream_t stream) {
-  if (!f || !R || !adjoint_out || !info_out || n_active < 1 || n_active > f->n_factored || !(tol > 0) ||
-      maxiter < 1) {
+  if (!f || !R || !adjoint_out || !info_out || !(tol > 0) || maxiter < 1) {
     set_last_error("orbit_adjoint_gmres_solve: bad arguments");
     return ORBIT_ERR_ARG;
   }
+  if (int rc0 = check_slots(f, n_active, true)) return rc0;
   std::lock_guard<std::mutex> lk(f->mu);
   return orbit_solve_impl(f, n_active, R, 1.0, lam_warm, tol, maxiter, restart, adjoint_out, info_out, 1,
                           (cudaStream_t)stream);

@@ -21,6 +21,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "common.cuh"
 #include "handles.h"
@@ -301,16 +302,20 @@ __global__ void k_update(FactorDev D, T* fronts, int64_t i0, int p0) {
     }
 }
 
-// Schur complement of a front: F22 -= L21 U12 (K = n), one 128 x 128 output
-// tile per CTA.  Register-tiled outer products (TM x TN per thread) from
-// shared-memory stages, with the next K slab prefetched into registers while
-// the current one is multiplied.
+// Register-tiled GEMM of one output tile: C (h x w) -= A (h x K) B (K x w), or
+// C = -A B when `assign`.  Each of 256 threads owns a TM x TN block of outputs;
+// the A and B slabs (128 x 16 and 16 x BN) go through shared memory with
+// 16-byte reads of the outer-product operands, and the next slab is prefetched
+// into registers while the current one is multiplied.
 template <typename T, int TM, int TN, int BN>
-__device__ __forceinline__ void schur_tile(const T* __restrict__ A, const T* __restrict__ B, T* C,
-                                           int ld, int K, int h, int w, T* As, T* Bs) {
+__device__ __forceinline__ void gemm_tile(const T* __restrict__ A, int lda, const T* __restrict__ B,
+                                          int ldb, T* C, int ldc, int K, int h, int w, bool assign,
+                                          T* As, T* Bs) {
   constexpr int BM = 128, BK = 16;
   constexpr int LDA = BM + 4, LDB = BN + 4;
   constexpr int AL = BM * BK / 256, BL = BK * BN / 256;
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int VW = 16 / sizeof(T);
   const int tid = threadIdx.x, tx = tid % (BN / TN), ty = tid / (BN / TN);
   T acc[TM][TN];
 #pragma unroll
@@ -322,12 +327,12 @@ __device__ __forceinline__ void schur_tile(const T* __restrict__ A, const T* __r
 #pragma unroll
     for (int q = 0; q < AL; ++q) {
       const int e = tid + q * 256, r = e / BK, kk = e % BK;
-      ra[q] = (r < h && k0 + kk < K) ? A[(int64_t)r * ld + k0 + kk] : T(0);
+      ra[q] = (r < h && k0 + kk < K) ? A[(int64_t)r * lda + k0 + kk] : T(0);
     }
 #pragma unroll
     for (int q = 0; q < BL; ++q) {
       const int e = tid + q * 256, kk = e / BN, c = e % BN;
-      rb[q] = (c < w && k0 + kk < K) ? B[(int64_t)(k0 + kk) * ld + c] : T(0);
+      rb[q] = (c < w && k0 + kk < K) ? B[(int64_t)(k0 + kk) * ldb + c] : T(0);
     }
   };
   load(0);
@@ -348,9 +353,23 @@ __device__ __forceinline__ void schur_tile(const T* __restrict__ A, const T* __r
     for (int kk = 0; kk < BK; ++kk) {
       T a[TM], b[TN];
 #pragma unroll
-      for (int i = 0; i < TM; ++i) a[i] = As[kk * LDA + ty * TM + i];
+      for (int i = 0; i < TM; i += VW) {
+        const V t = *reinterpret_cast<const V*>(As + kk * LDA + ty * TM + i);
+        if constexpr (sizeof(T) == 4) {
+          a[i] = t.x; a[i + 1] = t.y; a[i + 2] = t.z; a[i + 3] = t.w;
+        } else {
+          a[i] = t.x; a[i + 1] = t.y;
+        }
+      }
 #pragma unroll
-      for (int j = 0; j < TN; ++j) b[j] = Bs[kk * LDB + tx * TN + j];
+      for (int j = 0; j < TN; j += VW) {
+        const V t = *reinterpret_cast<const V*>(Bs + kk * LDB + tx * TN + j);
+        if constexpr (sizeof(T) == 4) {
+          b[j] = t.x; b[j + 1] = t.y; b[j + 2] = t.z; b[j + 3] = t.w;
+        } else {
+          b[j] = t.x; b[j + 1] = t.y;
+        }
+      }
 #pragma unroll
       for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -365,34 +384,87 @@ __device__ __forceinline__ void schur_tile(const T* __restrict__ A, const T* __r
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
       const int c = tx * TN + j;
-      if (c < w) C[(int64_t)r * ld + c] -= acc[i][j];
+      if (c < w) {
+        if (assign) C[(int64_t)r * ldc + c] = -acc[i][j];
+        else C[(int64_t)r * ldc + c] -= acc[i][j];
+      }
     }
   }
 }
 
+// C tile (128 x 128) -= / = - A B with K in [k0, K): FP32 as one 128x128
+// register tile, FP64 as two 128x64 halves.
+template <typename T>
+__device__ __forceinline__ void gemm_128(const T* A, int lda, const T* B, int ldb, T* C, int ldc, int K,
+                                         int h, int w, bool assign, T* smem) {
+  T* As = smem;
+  T* Bs = smem + 16 * (128 + 4);
+  if constexpr (sizeof(T) == 4) {
+    gemm_tile<T, 8, 8, 128>(A, lda, B, ldb, C, ldc, K, h, w, assign, As, Bs);
+  } else {
+    for (int half = 0; half < 2; ++half) {
+      const int cc = 64 * half;
+      if (cc >= w) break;
+      gemm_tile<T, 8, 4, 64>(A, lda, B + cc, ldb, C + cc, ldc, K, h, min(64, w - cc), assign, As, Bs);
+    }
+  }
+}
+
+// Schur complement of a front: F22 -= L21 U12 (K = n), one 128 x 128 tile per CTA.
 template <typename T>
 __global__ void __launch_bounds__(256) k_schur(FactorDev D, T* fronts, int64_t i0) {
   extern __shared__ unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);
+  T* sm = reinterpret_cast<T*>(smem_raw);
   const int4 it = D.items[i0 + blockIdx.x];
   const int s = it.x, tr = it.y, tc = it.z;
   const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
   T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   const int r0 = 128 * tr, c0 = 128 * tc;
-  const int h = min(128, m - r0);
-  const T* A = F + (int64_t)(n + r0) * ldf;
-  if constexpr (sizeof(T) == 4) {
-    T* Bs = As + 16 * (128 + 4);
-    schur_tile<T, 8, 8, 128>(A, F + n + c0, F + (int64_t)(n + r0) * ldf + n + c0, ldf, n, h,
-                             min(128, m - c0), As, Bs);
-  } else {
-    T* Bs = As + 16 * (128 + 4);
-    for (int half = 0; half < 2; ++half) {
-      const int cc = c0 + 64 * half;
-      if (cc >= m) break;
-      schur_tile<T, 8, 4, 64>(A, F + n + cc, F + (int64_t)(n + r0) * ldf + n + cc, ldf, n, h,
-                              min(64, m - cc), As, Bs);
+  gemm_128<T>(F + (int64_t)(n + r0) * ldf, ldf, F + n + c0, ldf, F + (int64_t)(n + r0) * ldf + n + c0, ldf, n,
+              min(128, m - r0), min(128, m - c0), false, sm);
+}
+
+// Dense copy of one triangle of the explicit inverses into the (no longer
+// needed) pivot block of the front: kind 0 -> unit-lower inv(L11), kind 1 ->
+// upper inv(U11), zeros elsewhere, so the panel products are plain GEMMs.
+template <typename T>
+__global__ void k_tri_copy(FactorDev D, T* fronts, const T* factors, int64_t i0, int kind, int inst_base) {
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, rb = it.y;
+  const int n = D.n[s], ldf = D.ldf[s], ldn = D.ldn[s];
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  const T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  for (int r = rb * 16 + (threadIdx.x >> 5); r < min(n, rb * 16 + 16); r += 8)
+    for (int c = threadIdx.x & 31; c < n; c += 32) {
+      T v;
+      if (kind == 0) v = c < r ? SQ[(int64_t)r * ldn + c] : (c == r ? T(1) : T(0));
+      else v = c >= r ? SQ[(int64_t)r * ldn + c] : T(0);
+      F[(int64_t)r * ldf + c] = v;
     }
+}
+
+// Panel products with the dense triangles in F11:
+// kind 0: Pb (m x n) = -L21 inv(L11), tile (tr of m, tc of n), K from 128 tc;
+// kind 1: Qr (n x m) = -inv(U11) U12, tile (tr of n, tc of m), K from 128 tr.
+template <typename T>
+__global__ void __launch_bounds__(256) k_prod2(FactorDev D, const T* fronts, T* factors, int64_t i0, int kind,
+                                               int inst_base) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, tr = it.y, tc = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s], ldm = D.ldm[s];
+  const T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  const int r0 = 128 * tr, c0 = 128 * tc;
+  if (kind == 0) {
+    T* Pb = SQ + (int64_t)n * ldn;
+    gemm_128<T>(F + (int64_t)(n + r0) * ldf + c0, ldf, F + (int64_t)c0 * ldf + c0, ldf, Pb + (int64_t)r0 * ldn + c0,
+                ldn, n - c0, min(128, m - r0), min(128, n - c0), true, sm);
+  } else {
+    T* Qr = SQ + (int64_t)(n + m) * ldn;
+    gemm_128<T>(F + (int64_t)r0 * ldf + r0, ldf, F + (int64_t)r0 * ldf + n + c0, ldf, Qr + (int64_t)r0 * ldm + c0,
+                ldm, n - r0, min(128, n - r0), min(128, m - c0), true, sm);
   }
 }
 
@@ -530,12 +602,13 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   D.group = f->front_group;
   T* factors = reinterpret_cast<T*>(f->factors);
   T* fronts = reinterpret_cast<T*>(f->fronts);
-  const int n_inst = n_active * 8;
+  const int n_inst = n_active * f->n_bins;
   const size_t sm_gemm = 2 * 16 * kLdS * sizeof(T);
   const size_t sm_inv = sm_gemm + 64 * kLdS * sizeof(T);
   const size_t sm_diag = 3 * 64 * kLdS * sizeof(T);
   const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
   ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_schur));
+  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_prod2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_schur));
   ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_diag));
   ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_inv));
   {
@@ -600,12 +673,22 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
           note_launch();
           break;
         }
-        case FactorLaunch::PROD: {
+        case FactorLaunch::TRIL:
+        case FactorLaunch::TRIU: {
           dim3 g((unsigned)L.items, G);
-          k_prod<T><<<g, kThreads, sm_gemm, st>>>(D, cur, factors, L.item_off, base);
+          k_tri_copy<T><<<g, 256, 0, st>>>(D, cur, factors, L.item_off, L.kind == FactorLaunch::TRIL ? 0 : 1, base);
           note_launch();
           break;
         }
+        case FactorLaunch::PRODL:
+        case FactorLaunch::PRODU: {
+          dim3 g((unsigned)L.items, G);
+          k_prod2<T><<<g, 256, sm_schur, st>>>(D, cur, factors, L.item_off, L.kind == FactorLaunch::PRODL ? 0 : 1, base);
+          note_launch();
+          break;
+        }
+        default:
+          break;
       }
       ORBIT_CUDA_TRY(cudaGetLastError());
     }

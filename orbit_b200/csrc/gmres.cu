@@ -241,10 +241,11 @@ __global__ void k_init_g(double* g, double* scal, const int* ids, int B) {
 // r = b - A x on the permuted 7-point stencil (FP64), trans: r = b - A^T x
 __global__ void k_stencil_resid(double* r, int64_t rs, const double* b, int64_t bs, const double* x,
                                 int64_t xs, const double* Ast, int tau, const int32_t* perm,
-                                const int32_t* iperm, int nz, int ny, int nx, int trans, const int* ids) {
+                                const int32_t* iperm, int nz, int ny, int nx, int trans, const int* ids,
+                                const int* set_of, int n_bins) {
   const int o = ids[blockIdx.y];
   const int64_t N = (int64_t)nz * ny * nx;
-  const double* A = Ast + ((int64_t)o * 8 + tau) * 7 * N;
+  const double* A = Ast + ((int64_t)set_of[o] * n_bins + tau) * 7 * N;
   const double* xv = x + (int64_t)o * xs;
   const double* bv = b + (int64_t)o * bs;
   double* rv = r + (int64_t)o * rs;
@@ -264,6 +265,38 @@ __global__ void k_stencil_resid(double* r, int64_t rs, const double* b, int64_t 
       acc = fma(a, xv[iperm[nb[d]]], acc);
     }
     rv[p] = bv[p] - acc;
+  }
+}
+
+// Block-cyclic residual of the eight bin equations A_tau c_{tau+1} = c_tau + fs e_tau
+// (c_0 := c_8):  R_tau = fs e_tau + c_tau - A_tau c_{tau+1}, FP64, permuted order.
+// C: per orbit 9 vectors (slot 0 unused, c_0 read from slot 8); E, R: per orbit 8 vectors.
+__global__ void k_block_resid(double* R, const double* E, double fs, const double* Cb, const double* Ast,
+                              const int32_t* perm, const int32_t* iperm, int nz, int ny, int nx,
+                              const int* ids, const int* set_of) {
+  const int o = ids[blockIdx.y];
+  const int64_t N = (int64_t)nz * ny * nx;
+  const int64_t nxy = (int64_t)nx * ny;
+  const double* C = Cb + (int64_t)o * 9 * N;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = perm[p];
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+    const int64_t nb[6] = {c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy};
+    const bool has[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+    int64_t q[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) q[d] = has[d] ? iperm[nb[d]] : 0;
+    for (int tau = 0; tau < 8; ++tau) {
+      const double* A = Ast + ((int64_t)set_of[o] * 8 + tau) * 7 * N;
+      const double* cin = C + (int64_t)(tau == 0 ? 8 : tau) * N;
+      const double* cout = C + (int64_t)(tau + 1) * N;
+      double acc = A[c] * cout[p];
+#pragma unroll
+      for (int d = 0; d < 6; ++d)
+        if (has[d]) acc = fma(A[(int64_t)(d + 1) * N + c], cout[q[d]], acc);
+      const double rhs = cin[p] + (E ? fs * E[((int64_t)o * 8 + tau) * N + p] : 0.0);
+      R[((int64_t)o * 8 + tau) * N + p] = rhs - acc;
+    }
   }
 }
 
@@ -370,7 +403,8 @@ int refined_bin(Ctx& c, const int* d_ids, int B, int tau, int tau1, const double
   k_lincomb<<<g, kVT, 0, c.st>>>(c.Tv, c.vs, one, XS + bin_out * N, xs, one, nullptr, 0, d_ids, N);
   note_launch();
   k_stencil_resid<<<g, kVT, 0, c.st>>>(c.Rv, c.vs, XS + bin_in * N, xs, c.Tv, c.vs, f->A_stencil, tau,
-                                       sy->d.perm, sy->d.iperm, sy->S.nz, sy->S.ny, sy->S.nx, trans, d_ids);
+                                       sy->d.perm, sy->d.iperm, sy->S.nz, sy->S.ny, sy->S.nx, trans, d_ids,
+                                       f->set_of, f->n_bins);
   note_launch();
   k_lincomb<<<g, kVT, 0, c.st>>>(XS + bin_in * N, xs, one, c.Rv, c.vs, one, nullptr, 0, d_ids, N);
   note_launch();
@@ -434,7 +468,8 @@ int matvec(Ctx& c, const double* v, int64_t vstride, double* w, int64_t wstride,
 // atol per orbit; iters accumulated; converged flags set.  rn_out gets the final true residual norm.
 int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<double>& atol,
           int maxiter, bool accurate_mv, std::vector<int>& iters, std::vector<int>& conv,
-          std::vector<double>& rn_out, std::vector<int>& matvecs, bool x_is_zero) {
+          std::vector<double>& rn_out, std::vector<int>& matvecs, bool x_is_zero,
+          bool trust_estimate = false) {
   orbit_factor_s* f = c.f;
   const int64_t N = c.N;
   const int R = c.R;
@@ -484,6 +519,8 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
     k_scale_inv_norm<<<vgrid(N, B), kVT, 0, c.st>>>(V_of(0), vstr, f->scal, S_NORM, d_ids, N);
     note_launch();
     std::vector<int> inner = act;
+    std::vector<char> est_done(f->n_orbits, 0);
+    std::vector<double> pres_h(f->n_orbits, 0.0);
     for (int o : act) ncol_h[o] = 0;
     for (int col = 0; col < R && !inner.empty(); ++col) {
       const int Bi = (int)inner.size();
@@ -531,7 +568,9 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
         ncol_h[o] = col + 1;
         const double pres = f->h_scal[o * kScal + S_PRES];
         const bool brk = f->h_scal[o * kScal + S_BREAK] != 0.0;
+        pres_h[o] = pres;
         if (!(pres <= atol[o] || brk)) keep.push_back(o);
+        else est_done[o] = 1;
       }
       inner.swap(keep);
     }
@@ -544,6 +583,23 @@ int gmres(Ctx& c, std::vector<int> act, double* b, double* x, const std::vector<
     note_launch();
     k_combine<<<vgrid(N, B), kVT, 0, c.st>>>(x, c.vs, f->V, vstr, f->red, 33, 0, d_ncol, 0, 1.0, d_ids, N);
     note_launch();
+    if (trust_estimate) {
+      // inner correction solves: accept the Arnoldi residual estimate
+      std::vector<int> rest;
+      for (int o : act) {
+        if (est_done[o]) {
+          conv[o] = 1;
+          rn_out[o] = pres_h[o];
+        } else {
+          rest.push_back(o);
+        }
+      }
+      act.swap(rest);
+      if (act.empty()) break;
+      B = (int)act.size();
+      rc = upload_ids(c, act, d_ids);
+      if (rc) return rc;
+    }
     // true residual r = b - A x -> V0 (unnormalised) and its norm
     rc = matvec(c, x, c.vs, c.Rv, c.vs, d_ids, B, accurate_mv);
     if (rc) return rc;
@@ -629,9 +685,109 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
     k_lincomb<<<g, kVT, 0, st>>>(c.Xv, c.vs, one, c.Sv, c.vs, zero, nullptr, 0, d_ids, N);
     note_launch();
   }
+  bool mixed_done = false;
   if (!c.mixed) {
     rc = gmres(c, act, c.Sv, c.Xv, atol, maxiter, false, iters, conv, rn, mv, false);
     if (rc) return rc;
+  } else if (!trans) {
+    // Block-cyclic FP64 refinement.  The orbit is the solution of the eight
+    // coupled bin equations A_tau c_{tau+1} = c_tau + dtau e_tau (c_0 := c_8);
+    // their FP64 residual needs only stencil products.  Each correction solves
+    // the same periodic problem with the residual as forcing, in FP32 (s_R by one
+    // chained sweep, GMRES on (I - M~), recovery sweep), and the FP64 orbit
+    // accumulates the corrections.  ||s_R|| is the reference's orbit residual
+    // ||(I - M) c_0 - s|| of the current orbit (orbit.py:196-199).
+    double* Cb = c.XS;                       // per orbit 9 vectors: c_1..c_8 in slots 1..8
+    double* Rb = f->tmpv + 15 * N * (int64_t)f->n_orbits;  // per orbit 8 vectors
+    ORBIT_CUDA_TRY(cudaMemsetAsync(Cb, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+    std::vector<int> oact = act;
+    if (warm && !oact.empty()) {
+      // start from the FP32 sweep of the warm start
+      const int B = (int)oact.size();
+      rc = upload_ids(c, oact, d_ids);
+      if (rc) return rc;
+      k_lincomb<<<vgrid(N, B), kVT, 0, st>>>(f->X, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
+      note_launch();
+      rc = launch_chain(f, B, d_ids, 0, 0, 8, f->E, dtau, st);
+      if (rc) return rc;
+      for (int t = 1; t <= 8; ++t) {
+        k_lincomb<<<vgrid(N, B), kVT, 0, st>>>(Cb + t * N, 9 * N, one, f->X + t * N, 9 * N, zero, nullptr, 0,
+                                               d_ids, N);
+        note_launch();
+      }
+      for (int o : oact) mv[o]++;
+    }
+    const int max_outer = 8;
+    for (int it = 0; it <= max_outer && !oact.empty(); ++it) {
+      const int B = (int)oact.size();
+      rc = upload_ids(c, oact, d_ids);
+      if (rc) return rc;
+      const dim3 gb = vgrid(N, B);
+      k_block_resid<<<gb, kVT, 0, st>>>(Rb, f->E, dtau, Cb, f->A_stencil, sy->d.perm, sy->d.iperm, sy->S.nz,
+                                        sy->S.ny, sy->S.nx, d_ids, f->set_of);
+      note_launch();
+      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+      rc = launch_chain(f, B, d_ids, 0, 0, 8, Rb, 1.0, st);
+      if (rc) return rc;
+      for (int o : oact) mv[o]++;
+      k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, f->X + 8 * N, 9 * N, zero, nullptr, 0, d_ids, N);
+      note_launch();
+      rc = sqnorm(c, c.Dv, c.vs, d_ids, B, S_TMP);
+      if (rc) return rc;
+      rc = fetch_scal(c);
+      if (rc) return rc;
+      std::vector<int> keep;
+      std::vector<double> itol(f->n_orbits, 0.0);
+      for (int o : oact) {
+        const double r = std::sqrt(std::max(f->h_scal[o * kScal + S_TMP], 0.0));
+        rn[o] = r;
+        if (r <= atol[o]) {
+          conv[o] = 1;
+        } else if (it < max_outer) {
+          keep.push_back(o);
+          itol[o] = std::max(atol[o] * 0.5, 1e-4 * r);
+        }
+      }
+      oact.swap(keep);
+      if (oact.empty()) break;
+      const int B2 = (int)oact.size();
+      rc = upload_ids(c, oact, d_ids);
+      if (rc) return rc;
+      double* xcorr = f->tmpv + 5 * N;
+      k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(xcorr, c.vs, zero, nullptr, 0, zero, nullptr, 0, d_ids, N);
+      note_launch();
+      std::vector<int> cin(f->n_orbits, 0);
+      std::vector<double> rin(f->n_orbits, 0.0);
+      rc = gmres(c, oact, c.Dv, xcorr, itol, maxiter, false, iters, cin, rin, mv, true, true);
+      if (rc) return rc;
+      rc = upload_ids(c, oact, d_ids);
+      if (rc) return rc;
+      // corrections of every bin: recovery sweep from delta_0 with the residual forcing
+      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+      k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(f->X, 9 * N, one, xcorr, c.vs, zero, nullptr, 0, d_ids, N);
+      note_launch();
+      rc = launch_chain(f, B2, d_ids, 0, 0, 8, Rb, 1.0, st);
+      if (rc) return rc;
+      for (int o : oact) mv[o]++;
+      for (int t = 1; t <= 8; ++t) {
+        k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(Cb + t * N, 9 * N, one, Cb + t * N, 9 * N, one, f->X + t * N,
+                                                9 * N, d_ids, N);
+        note_launch();
+      }
+      for (int o : oact) outer[o]++;
+    }
+    // orbit [c_8, c_1, ..., c_8] into the chain buffer
+    rc = upload_ids(c, all, d_ids);
+    if (rc) return rc;
+    for (int t = 0; t <= 8; ++t) {
+      k_lincomb<<<g, kVT, 0, st>>>(f->X + t * N, 9 * N, one, Cb + (t == 0 ? 8 : t) * N, 9 * N, zero, nullptr,
+                                   0, d_ids, N);
+      note_launch();
+    }
+    // periodicity of the exact sweep from c_0: ||c_8' - c_0|| = ||(I - M) c_0 - s||
+    k_lincomb<<<g, kVT, 0, st>>>(c.Tv, c.vs, one, c.Dv, c.vs, zero, nullptr, 0, d_ids, N);
+    note_launch();
+    mixed_done = true;
   } else {
     // outer FP64 refinement of the monodromy residual
     std::vector<int> oact = act;
@@ -688,6 +844,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   // recovery: chain with forcing from x
   rc = upload_ids(c, all, d_ids);
   if (rc) return rc;
+  if (!mixed_done) {
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * n, st));
   k_lincomb<<<g, kVT, 0, st>>>(f->X + in * N, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
   note_launch();
@@ -699,9 +856,10 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
     rc = chain_accurate(c, d_ids, n, f->E, fscale, 1, 8);
     if (rc) return rc;
     // X[tau] for tau = 2..7 hold P^T(...) without R: add R_tau (X[1] already has it)
-    for (int t = 2; t < 8; ++t)
+    for (int t = 2; t < 8; ++t) {
       k_lincomb<<<g, kVT, 0, st>>>(f->X + t * N, 9 * N, one, f->X + t * N, 9 * N, one, f->E + t * N, 8 * N, d_ids, N);
       note_launch();
+    }
   }
   for (int o = 0; o < n; ++o) mv[o]++;
   // periodicity: forward ||X8 - X0|| / (||X0|| + 1e-30); adjoint: ||P0^T lam1 + R0 - lam0|| / ...
@@ -720,6 +878,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
     note_launch();
     k_lincomb<<<g, kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
     note_launch();
+  }
   }
   rc = sqnorm(c, c.Tv, c.vs, d_ids, n, S_TMP);
   if (rc) return rc;

@@ -23,6 +23,7 @@ struct DevSym {
   int32_t *phase_off = nullptr, *phase_offT = nullptr;
   int32_t *nchunk_fwd = nullptr, *nchunk_bwd = nullptr, *nchunk_fwdT = nullptr, *nchunk_bwdT = nullptr;
   int32_t *perm = nullptr, *iperm = nullptr;
+  int32_t *level = nullptr;
 };
 
 struct orbit_symbolic_s {
@@ -36,7 +37,11 @@ struct orbit_symbolic_s {
 
 struct orbit_factor_s {
   orbit_symbolic_s* sym = nullptr;
-  int n_orbits = 0;
+  int n_orbits = 0;   // solve slots (vectors, counters)
+  int n_sets = 0;     // factor sets (each n_bins factorizations)
+  int n_bins = 8;     // 8, or 1 for a single-factor handle
+  int* set_of = nullptr;           // device: factor set of each solve slot
+  std::vector<int> h_set_of;       // host mirror
   int precision = 64;
   int device = 0;
   int n_factored = 0;

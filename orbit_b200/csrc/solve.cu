@@ -19,6 +19,8 @@
 // leaves the loop.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "handles.h"
 
@@ -26,13 +28,20 @@ namespace orbit {
 
 namespace {
 
-constexpr int kSolveThreads = 256;
+#ifndef ORBIT_SOLVE_THREADS
+#define ORBIT_SOLVE_THREADS 128
+#endif
+#ifndef ORBIT_SOLVE_MINB
+#define ORBIT_SOLVE_MINB 8
+#endif
+constexpr int kSolveThreads = ORBIT_SOLVE_THREADS;
 constexpr int kWarps = kSolveThreads / 32;
 
 template <typename T>
 struct ChainDev {
   const int32_t *first, *n, *m, *parent, *child, *uidx, *rel, *ldn, *ldm;
-  const int32_t *nch_f, *nch_b;
+  const int32_t *nch_f, *nch_b, *level;
+  int sub_front;  // per-warp vector capacity for subtree tasks
   const int64_t *uoff, *fac_off, *woff;
   const int4* items;
   const int32_t* phase_off;
@@ -48,6 +57,8 @@ struct ChainDev {
   int* task_counter;
   int* status;
   const int* orbit_ids;
+  const int* set_of;  // factor set of each solve slot
+  int n_bins;
   int B, tau0, tau1, trans;
   int total;
   long long spin_limit;
@@ -55,30 +66,62 @@ struct ChainDev {
 
 __device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit) {
   long long it = 0;
+  unsigned ns = 32;
   while (ld_acquire(p) < target) {
     if (ld_volatile(status) != 0) return false;
     if (++it > limit) {
       raise_status(status, ORBIT_ERR_TIMEOUT);
       return false;
     }
-    __nanosleep(100);
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
   }
   return true;
 }
 
+// Vector types for 16-byte loads of factor rows (rows start 16-byte aligned:
+// every leading dimension and block offset is a multiple of 4 elements).
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int w = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int w = 2; };
+
+__device__ __forceinline__ float dot16(const float4& a, const float* v) {
+  return a.x * v[0] + a.y * v[1] + a.z * v[2] + a.w * v[3];
+}
+__device__ __forceinline__ double dot16(const double2& a, const double* v) {
+  return a.x * v[0] + a.y * v[1];
+}
+
+// Per-lane partial of sum_{j0 <= j < j1} a[j] v[j] (a 16-byte aligned at j = 0,
+// v in shared memory, 16-byte aligned); 16-byte loads, four in flight per lane.
+template <typename T>
+__device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0, int j1, int lane) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::w;
+  T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
+  // [j0, ja) scalar head up to the first aligned index, [ja, jb) 16-byte
+  // vectors, [jb, j1) scalar tail
+  const int ja = min((j0 + W - 1) / W * W, j1);
+  const int jb = max(ja, j1 / W * W);
+  for (int j = j0 + lane; j < ja; j += 32) acc0 = fma(__ldg(a + j), v[j], acc0);
+  const int nv0 = ja / W, nv1 = jb / W;
+  const V* a4 = reinterpret_cast<const V*>(a);
+  int k = nv0 + lane;
+  for (; k + 96 < nv1; k += 128) {
+    const V x0 = __ldg(a4 + k), x1 = __ldg(a4 + k + 32), x2 = __ldg(a4 + k + 64), x3 = __ldg(a4 + k + 96);
+    acc0 += dot16(x0, v + k * W);
+    acc1 += dot16(x1, v + (k + 32) * W);
+    acc2 += dot16(x2, v + (k + 64) * W);
+    acc3 += dot16(x3, v + (k + 96) * W);
+  }
+  for (; k < nv1; k += 32) acc0 += dot16(__ldg(a4 + k), v + k * W);
+  for (int j = jb + lane; j < j1; j += 32) acc1 = fma(__ldg(a + j), v[j], acc1);
+  return (acc0 + acc1) + (acc2 + acc3);
+}
+
 template <typename T>
 __device__ __forceinline__ T dot_row(const T* __restrict__ a, const T* v, int len, int lane) {
-  T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
-  int j = lane;
-  for (; j + 96 < len; j += 128) {
-    T a0 = __ldg(a + j), a1 = __ldg(a + j + 32), a2 = __ldg(a + j + 64), a3 = __ldg(a + j + 96);
-    acc0 = fma(a0, v[j], acc0);
-    acc1 = fma(a1, v[j + 32], acc1);
-    acc2 = fma(a2, v[j + 64], acc2);
-    acc3 = fma(a3, v[j + 96], acc3);
-  }
-  for (; j < len; j += 32) acc0 = fma(__ldg(a + j), v[j], acc0);
-  return warp_sum((acc0 + acc1) + (acc2 + acc3));
+  return warp_sum(dot_seg(a, v, 0, len, lane));
 }
 
 // Forward step of one supernode (L, or U^T when trans) for output rows
@@ -92,7 +135,7 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
   const int64_t N = D.N;
   const int n = D.n[s], m = D.m[s], first = D.first[s];
   const int ldn = D.ldn[s], ldm = D.ldm[s];
-  const T* SQ = D.factors + (int64_t)(o * 8 + tau) * D.fac_size + D.fac_off[s];
+  const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
   double* Yo = D.Y + (int64_t)o * N;
   double* Wo = D.W + (int64_t)o * D.w_size;
   const int bin_in = trans ? tau + 1 : tau;
@@ -160,7 +203,9 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
 }
 
 // Backward step of one supernode (U, or L^T when trans) for rows [r0, r1):
-// own forward result plus the ancestors' solution.  Ends with a block barrier.
+// own forward result plus the ancestors' solution; the ancestor part of `vec`
+// starts at the next 4-element boundary after the own part so both segments
+// can be read with 16-byte loads.  Ends with a block barrier.
 template <typename T>
 __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
                          T* vec, T* red) {
@@ -168,36 +213,32 @@ __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
   const int64_t N = D.N;
   const int n = D.n[s], m = D.m[s], first = D.first[s];
   const int ldn = D.ldn[s], ldm = D.ldm[s];
-  const T* SQ = D.factors + (int64_t)(o * 8 + tau) * D.fac_size + D.fac_off[s];
+  const int n0pad = (n + 3) & ~3;
+  const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
   const double* Yo = D.Y + (int64_t)o * N;
   const int bin_out = trans ? tau : tau + 1;
   double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
   const int32_t* ui = D.uidx + D.uoff[s];
-  for (int i = tid; i < n + m; i += kSolveThreads) vec[i] = (T)(i < n ? Yo[first + i] : Xout[ui[i - n]]);
+  for (int i = tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
+  for (int u = tid; u < m; u += kSolveThreads) vec[n0pad + u] = (T)Xout[ui[u]];
   __syncthreads();
   if (!trans) {
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
     for (int i = r0 + warp; i < r1; i += kWarps) {
-      const T* row = SQ + (int64_t)i * ldn;
-      T acc0 = T(0), acc1 = T(0);
-      for (int j = i + lane; j < n; j += 32) acc0 = fma(__ldg(row + j), vec[j], acc0);
-      const T* qrow = Qr + (int64_t)i * ldm;
-      int j = lane;
-      for (; j + 32 < m; j += 64) {
-        acc1 = fma(__ldg(qrow + j), vec[n + j], acc1);
-        acc0 = fma(__ldg(qrow + j + 32), vec[n + j + 32], acc0);
-      }
-      for (; j < m; j += 32) acc1 = fma(__ldg(qrow + j), vec[n + j], acc1);
-      T acc = warp_sum(acc0 + acc1);
+      T acc = dot_seg(SQ + (int64_t)i * ldn, vec, i, n, lane);
+      acc += dot_seg(Qr + (int64_t)i * ldm, vec + n0pad, 0, m, lane);
+      acc = warp_sum(acc);
       if (lane == 0) Xout[first + i] = (double)acc;
     }
   } else {
     // columns of [SQ_strict_lower ; Pb] with unit diagonal
+    const T* Pb = SQ + (int64_t)n * ldn;
     for (int cb = r0; cb < r1; cb += 32) {
       const int c = cb + lane;
       T acc = T(0);
       if (c < r1) {
-        for (int i = c + 1 + warp; i < n + m; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
+        for (int i = c + 1 + warp; i < n; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
+        for (int u = warp; u < m; u += kWarps) acc = fma(__ldg(Pb + (int64_t)u * ldn + c), vec[n0pad + u], acc);
       }
       red[warp * 32 + lane] = acc;
       __syncthreads();
@@ -213,8 +254,117 @@ __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
   __syncthreads();
 }
 
+// Warp-level forward step of one small supernode (inside a subtree task).
 template <typename T>
-__global__ void __launch_bounds__(kSolveThreads) k_chain(ChainDev<T> D) {
+__device__ void fwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool trans, T* v) {
+  const int lane = threadIdx.x & 31;
+  const int64_t N = D.N;
+  const int n = D.n[s], m = D.m[s], first = D.first[s];
+  const int ldn = D.ldn[s], ldm = D.ldm[s];
+  const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+  double* Yo = D.Y + (int64_t)o * N;
+  double* Wo = D.W + (int64_t)o * D.w_size;
+  const int bin_in = trans ? tau + 1 : tau;
+  const double* Xin = D.X + ((int64_t)o * 9 + bin_in) * N;
+  const double* Ein = nullptr;
+  if (D.E) {
+    if (!trans) Ein = D.E + ((int64_t)o * 8 + tau) * N;
+    else if (tau + 1 < D.tau1) Ein = D.E + ((int64_t)o * 8 + tau + 1) * N;
+  }
+  for (int i = lane; i < n + m; i += 32) {
+    double x = 0.0;
+    if (i < n) {
+      x = Xin[first + i];
+      if (Ein) x += D.escale * Ein[first + i];
+    }
+    v[i] = (T)x;
+  }
+  for (int q2 = 0; q2 < 2; ++q2) {
+    __syncwarp();
+    const int c = D.child[2 * s + q2];
+    if (c < 0) continue;
+    const int mc = D.m[c];
+    const int32_t* rel = D.rel + D.uoff[c];
+    const double* wc = Wo + D.woff[c];
+    for (int j = lane; j < mc; j += 32) v[rel[j]] += (T)wc[j];
+  }
+  __syncwarp();
+  const int64_t woff = D.woff[s];
+  if (!trans) {
+    if (n <= 64) {
+      for (int i = lane; i < n + m; i += 32) {
+        const int len = i < n ? i : n;
+        const T* row = SQ + (int64_t)i * ldn;
+        T acc = T(0);
+        for (int j = 0; j < len; ++j) acc = fma(__ldg(row + j), v[j], acc);
+        if (i < n) Yo[first + i] = (double)(v[i] + acc);
+        else Wo[woff + (i - n)] = (double)(v[i] + acc);
+      }
+    } else {
+      for (int i = 0; i < n + m; ++i) {
+        const int len = i < n ? i : n;
+        T acc = dot_row(SQ + (int64_t)i * ldn, v, len, lane);
+        if (lane == 0) {
+          if (i < n) Yo[first + i] = (double)(v[i] + acc);
+          else Wo[woff + (i - n)] = (double)(v[i] + acc);
+        }
+      }
+    }
+  } else {
+    const T* Qr = SQ + (int64_t)(n + m) * ldn;
+    for (int c = lane; c < n + m; c += 32) {
+      T acc = T(0);
+      if (c < n) {
+        for (int i = 0; i <= c; ++i) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), v[i], acc);
+        Yo[first + c] = (double)acc;
+      } else {
+        const int u = c - n;
+        for (int i = 0; i < n; ++i) acc = fma(__ldg(Qr + (int64_t)i * ldm + u), v[i], acc);
+        Wo[woff + u] = (double)(v[c] + acc);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Warp-level backward step of one small supernode (inside a subtree task).
+template <typename T>
+__device__ void bwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool trans, T* v) {
+  const int lane = threadIdx.x & 31;
+  const int64_t N = D.N;
+  const int n = D.n[s], m = D.m[s], first = D.first[s];
+  const int ldn = D.ldn[s], ldm = D.ldm[s];
+  const int n0pad = (n + 3) & ~3;
+  const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+  const double* Yo = D.Y + (int64_t)o * N;
+  const int bin_out = trans ? tau : tau + 1;
+  double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
+  const int32_t* ui = D.uidx + D.uoff[s];
+  for (int i = lane; i < n; i += 32) v[i] = (T)Yo[first + i];
+  for (int u = lane; u < m; u += 32) v[n0pad + u] = (T)Xout[ui[u]];
+  __syncwarp();
+  if (!trans) {
+    const T* Qr = SQ + (int64_t)(n + m) * ldn;
+    for (int i = 0; i < n; ++i) {
+      T acc = dot_seg(SQ + (int64_t)i * ldn, v, i, n, lane);
+      acc += dot_seg(Qr + (int64_t)i * ldm, v + n0pad, 0, m, lane);
+      acc = warp_sum(acc);
+      if (lane == 0) Xout[first + i] = (double)acc;
+    }
+  } else {
+    const T* Pb = SQ + (int64_t)n * ldn;
+    for (int c = lane; c < n; c += 32) {
+      T acc = v[c];
+      for (int i = c + 1; i < n; ++i) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), v[i], acc);
+      for (int u = 0; u < m; ++u) acc = fma(__ldg(Pb + (int64_t)u * ldn + c), v[n0pad + u], acc);
+      Xout[first + c] = (double)acc;
+    }
+  }
+  __syncwarp();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(ChainDev<T> D) {
   extern __shared__ unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);      // kWarps * 32
   T* vec = red + kWarps * 32;                    // front-sized vector
@@ -273,13 +423,27 @@ __global__ void __launch_bounds__(kSolveThreads) k_chain(ChainDev<T> D) {
     if (!subtree) {
       if (fwd) fwd_node(D, o, tau, s, it.y, it.z, trans, vec, red);
       else bwd_node(D, o, tau, s, it.y, it.z, trans, vec, red);
-    } else if (fwd) {
-      // postorder: every child before its parent
-      for (int d = it.y; d <= s; ++d)
-        fwd_node(D, o, tau, d, 0, trans ? D.n[d] + D.m[d] : D.n[d] + D.m[d], trans, vec, red);
     } else {
-      // reverse postorder: every parent before its children
-      for (int d = s; d >= it.y; --d) bwd_node(D, o, tau, d, 0, D.n[d], trans, vec, red);
+      // Whole subtree in this CTA: depth by depth (deepest first for the
+      // forward sweep, root first for the backward sweep), the supernodes of
+      // one depth spread over the warps, one warp per supernode.
+      const int warp = threadIdx.x >> 5;
+      T* wv = vec + warp * ((D.sub_front + 7) & ~3);
+      const int d0 = it.y;
+      const int top = D.level[s];
+      int deep = top;
+      for (int d = d0; d <= s; ++d) deep = max(deep, D.level[d]);
+      for (int q3 = 0; q3 <= deep - top; ++q3) {
+        const int lev = fwd ? deep - q3 : top + q3;
+        int k = 0;
+        for (int d = d0; d <= s; ++d) {
+          if (D.level[d] != lev) continue;
+          if ((k++ & (kWarps - 1)) != warp) continue;
+          if (fwd) fwd_node_warp(D, o, tau, d, trans, wv);
+          else bwd_node_warp(D, o, tau, d, trans, wv);
+        }
+        __syncthreads();
+      }
     }
     if (tid == 0) {
       __threadfence();
@@ -308,6 +472,8 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.child = sy->d.child; D.uidx = sy->d.uidx; D.rel = sy->d.rel; D.ldn = sy->d.ldn; D.ldm = sy->d.ldm;
   D.nch_f = trans ? sy->d.nchunk_fwdT : sy->d.nchunk_fwd;
   D.nch_b = trans ? sy->d.nchunk_bwdT : sy->d.nchunk_bwd;
+  D.level = sy->d.level;
+  D.sub_front = S.max_sub_front;
   D.uoff = sy->d.uoff; D.fac_off = sy->d.fac_off; D.woff = sy->d.woff;
   D.items = trans ? sy->d.sitems + S.items_per_bin : sy->d.sitems;
   D.phase_off = trans ? sy->d.phase_offT : sy->d.phase_off;
@@ -319,13 +485,16 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.X = X; D.E = E; D.escale = escale; D.Y = f->Ybuf; D.W = f->Wbuf;
   D.counters = f->counters; D.task_counter = f->task_counter; D.status = f->status;
   D.orbit_ids = d_orbit_ids; D.B = B; D.tau0 = tau0; D.tau1 = tau1; D.trans = trans;
+  D.set_of = f->set_of; D.n_bins = f->n_bins;
   D.total = (tau1 - tau0) * D.items_per_bin * B;
-  D.spin_limit = 4000000LL;  // bounded: a few seconds of 100 ns sleeps
+  D.spin_limit = 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
   if (D.total <= 0) return ORBIT_OK;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->counters, 0, sizeof(int) * (size_t)f->n_orbits * 16 * S.nsuper, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
-  const size_t smem = sizeof(T) * ((size_t)kWarps * 32 + S.max_front + 8);
+  const size_t smem =
+      sizeof(T) * ((size_t)kWarps * 32 + std::max<size_t>(S.max_front + 8, (size_t)kWarps * ((S.max_sub_front + 7) & ~3)) + 8);
   ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_chain<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_chain<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, sms = 0, occ = 0;
   ORBIT_CUDA_TRY(cudaGetDevice(&dev));
   ORBIT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

@@ -338,15 +338,29 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
       }
       if (nitems() > off) S.fsched.push_back({FactorLaunch::INV, l, t * kNB, off, nitems() - off});
     }
-    int64_t off = nitems();
-    for (int s : sups) {
-      int tn = (S.n[s] + kTile - 1) / kTile, tm = (S.m[s] + kTile - 1) / kTile;
-      for (int a = 0; a < tm; ++a)
-        for (int b = 0; b < tn; ++b) push_item(s, 0, a, b);  // Pb tile (rows of m, cols of n)
-      for (int a = 0; a < tn; ++a)
-        for (int b = 0; b < tm; ++b) push_item(s, 1, a, b);  // Qr tile (rows of n, cols of m)
+    // panel products via dense triangles copied into the pivot block
+    for (int which = 0; which < 2; ++which) {
+      int64_t off = nitems();
+      for (int s : sups)
+        if (S.m[s] > 0)
+          for (int rb = 0; rb * 16 < S.n[s]; ++rb) push_item(s, rb, 0, 0);
+      if (nitems() > off)
+        S.fsched.push_back({which == 0 ? FactorLaunch::TRIL : FactorLaunch::TRIU, l, 0, off, nitems() - off});
+      off = nitems();
+      for (int s : sups) {
+        const int tn = (S.n[s] + kSchurTile - 1) / kSchurTile, tm = (S.m[s] + kSchurTile - 1) / kSchurTile;
+        if (S.m[s] == 0) continue;
+        if (which == 0) {
+          for (int a = 0; a < tm; ++a)
+            for (int b = 0; b < tn; ++b) push_item(s, a, b, 0);  // Pb tile (rows of m, cols of n)
+        } else {
+          for (int a = 0; a < tn; ++a)
+            for (int b = 0; b < tm; ++b) push_item(s, a, b, 0);  // Qr tile (rows of n, cols of m)
+        }
+      }
+      if (nitems() > off)
+        S.fsched.push_back({which == 0 ? FactorLaunch::PRODL : FactorLaunch::PRODU, l, 0, off, nitems() - off});
     }
-    if (nitems() > off) S.fsched.push_back({FactorLaunch::PROD, l, 0, off, nitems() - off});
   }
 
   // ---- solve schedule ----
@@ -397,6 +411,9 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     if (p >= 0 && S.role[p] != 0) S.role[s] = 2;
     else if (subw[s] <= wmax && (S.nchild[s] > 0 || p < 0 || subw[p] > wmax)) S.role[s] = 1;
   }
+  S.max_sub_front = 0;
+  for (int s2 = 0; s2 < ns; ++s2)
+    if (S.role[s2] != 0) S.max_sub_front = std::max(S.max_sub_front, S.n[s2] + S.m[s2]);
   auto push4 = [&](int a, int b, int c, int d) {
     S.sitems.push_back(a); S.sitems.push_back(b); S.sitems.push_back(c); S.sitems.push_back(d);
   };

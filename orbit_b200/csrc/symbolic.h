@@ -29,7 +29,7 @@ inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 // One kernel launch of the numeric factorization schedule.
 struct FactorLaunch {
-  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, PROD } kind;
+  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU } kind;
   int level;
   int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV)
   int64_t item_off;  // offset into the item array (int4 units)
@@ -81,6 +81,7 @@ struct Symbolic {
   std::vector<int32_t> nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT;
   std::vector<int32_t> role;  // 0 chunked node, 1 subtree-task root, 2 inside a subtree
   int max_front = 0;
+  int max_sub_front = 0;  // largest n+m of a supernode inside a subtree task
   int max_nm = 0;
   double factor_flops = 0.0;
 };

@@ -123,29 +123,40 @@ class FactorBatch:
     """n_orbits x 8 numeric factorizations sharing a Symbolic, plus the chained
     solves and the periodic-orbit GMRES that run on them."""
 
-    def __init__(self, sym: Symbolic, n_orbits: int, precision: int = 64):
+    def __init__(self, sym: Symbolic, n_orbits: int, precision: int = 64,
+                 n_sets: Optional[int] = None, n_bins: int = N_BINS):
         _require_cuda()
         self.sym = sym
         self.n_orbits = int(n_orbits)
+        self.n_sets = int(n_sets) if n_sets is not None else self.n_orbits
+        self.n_bins = int(n_bins)
         self.precision = int(precision)
         h = C.c_void_p()
-        _lib.check(_lib.lib().orbit_factor_create(sym.handle, self.n_orbits, self.precision,
-                                                  C.byref(h)))
+        _lib.check(_lib.lib().orbit_factor_create_ex(sym.handle, self.n_orbits, self.n_sets, self.n_bins,
+                                                     self.precision, C.byref(h)))
         self._h = h
         self.n_factored = 0
         self.N = sym.N
 
+    def map(self, set_of_orbit: Sequence[int]):
+        """Factor set of each solve slot (many right-hand sides may share one set)."""
+        a = np.ascontiguousarray(np.asarray(set_of_orbit, dtype=np.int32))
+        if a.shape != (self.n_orbits,):
+            raise ValueError(f"need {self.n_orbits} set indices")
+        _lib.check(_lib.lib().orbit_factor_map(self._h, a.ctypes.data))
+
     def numeric(self, T_stencils: Sequence[torch.Tensor], sinks: Optional[Sequence[torch.Tensor]],
                 dtau: float = DTAU):
-        """Factor len(T_stencils)//8 orbits; lists are orbit-major, bin-minor."""
+        """Factor len(T_stencils)//n_bins factor sets; lists are set-major, bin-minor."""
         n_inst = len(T_stencils)
-        if n_inst % N_BINS or n_inst // N_BINS > self.n_orbits:
-            raise ValueError("need 8 stencils per orbit, at most n_orbits orbits")
+        nb = self.n_bins
+        if n_inst % nb or n_inst // nb > self.n_sets:
+            raise ValueError(f"need {nb} stencils per factor set, at most {self.n_sets} sets")
         tp = _lib.ptr_array([_lib.ptr(t) for t in T_stencils])
         dp = _lib.ptr_array([_lib.ptr(d) for d in sinks]) if sinks is not None else None
-        _lib.check(_lib.lib().orbit_factor_numeric(self._h, n_inst // N_BINS, tp, dp, float(dtau),
+        _lib.check(_lib.lib().orbit_factor_numeric(self._h, n_inst // nb, tp, dp, float(dtau),
                                                    _stream()))
-        self.n_factored = n_inst // N_BINS
+        self.n_factored = n_inst // nb
         self.dtau = float(dtau)
 
     def chain(self, x: torch.Tensor, trans: bool = False, tau0: int = 0, tau1: int = N_BINS,
@@ -154,6 +165,8 @@ class FactorBatch:
         x = x.reshape(-1, self.N).contiguous()
         n = x.shape[0]
         out = torch.empty_like(x)
+        if tau1 > self.n_bins:
+            tau1 = self.n_bins
         f = forcing.reshape(n, N_BINS, self.N).contiguous() if forcing is not None else None
         _lib.check(_lib.lib().orbit_chain_apply(self._h, n, int(trans), int(tau0), int(tau1),
                                                 _lib.ptr(x), _lib.ptr(out), _lib.ptr(f), float(fscale),

@@ -19,7 +19,8 @@ from . import _lib
 _INT64_ARRAYS = {"uoff", "fac_off", "front_off", "level_front_size", "ent_level_off", "ent_pos", "woff"}
 
 INFO_KEYS = ("N", "nsuper", "nlevels", "factor_nnz", "factor_elems", "front_elems", "max_front",
-             "factor_flops", "solve_items_per_bin", "update_len", "leaf_cells", "max_nm")
+             "factor_flops", "solve_items_per_bin", "update_len", "leaf_cells", "max_nm",
+             "max_sub_front")
 
 
 class Symbolic:
@@ -30,8 +31,8 @@ class Symbolic:
         self._h = h
         self.nz, self.ny, self.nx = int(nz), int(ny), int(nx)
         self.N = self.nz * self.ny * self.nx
-        buf = (C.c_int64 * 12)()
-        _lib.check(L.orbit_symbolic_info(h, buf, 12))
+        buf = (C.c_int64 * 13)()
+        _lib.check(L.orbit_symbolic_info(h, buf, 13))
         self.info = {k: int(buf[i]) for i, k in enumerate(INFO_KEYS)}
 
     @property
