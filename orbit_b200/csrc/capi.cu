@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <set>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -18,6 +20,23 @@ static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 static std::atomic<long long> g_launches{0};
 void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int allow_max_smem(const void* func) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  ORBIT_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({func, dev})) return ORBIT_OK;
+  int optin = 0;
+  ORBIT_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  ORBIT_CUDA_TRY(cudaFuncGetAttributes(&fa, func));
+  ORBIT_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      optin - (int)fa.sharedSizeBytes));
+  done.insert({func, dev});
+  return ORBIT_OK;
+}
 
 int run_factor(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st);
 int launch_chain(orbit_factor_s* f, int B, const int* d_orbit_ids, int trans, int tau0, int tau1,

@@ -11,6 +11,10 @@ namespace orbit {
 void set_last_error(const std::string& msg);
 // Count of kernels this library has launched (all handles, all threads).
 void note_launch(int n = 1);
+// Raise a kernel's dynamic shared-memory limit to the device's opt-in maximum,
+// once per (kernel, device).  The limit is per-function state shared by every
+// thread, so it is only ever raised, never set per call.
+int allow_max_smem(const void* func);
 
 #define ORBIT_CUDA_TRY(expr)                                                     \
   do {                                                                           \

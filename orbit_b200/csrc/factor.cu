@@ -607,10 +607,10 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   const size_t sm_inv = sm_gemm + 64 * kLdS * sizeof(T);
   const size_t sm_diag = 3 * 64 * kLdS * sizeof(T);
   const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
-  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_schur));
-  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_prod2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_schur));
-  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_diag));
-  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_inv));
+  { int _r = allow_max_smem((const void*)k_schur<T>); if (_r) return _r; }
+  { int _r = allow_max_smem((const void*)k_prod2<T>); if (_r) return _r; }
+  { int _r = allow_max_smem((const void*)k_diag<T>); if (_r) return _r; }
+  { int _r = allow_max_smem((const void*)k_inv<T>); if (_r) return _r; }
   {
     dim3 g(clamp_grid((7 * S.N + 255) / 256), n_inst);
     k_copy_A<<<g, 256, 0, st>>>(f->A_stencil, f->d_Tptr, f->d_Dptr, 0, S.N, dtau);

@@ -493,8 +493,10 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
   const size_t smem =
       sizeof(T) * ((size_t)kWarps * 32 + std::max<size_t>(S.max_front + 8, (size_t)kWarps * ((S.max_sub_front + 7) & ~3)) + 8);
-  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_chain<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ORBIT_CUDA_TRY(cudaFuncSetAttribute(k_chain<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  {
+    int r0 = allow_max_smem((const void*)k_chain<T>);
+    if (r0) return r0;
+  }
   int dev = 0, sms = 0, occ = 0;
   ORBIT_CUDA_TRY(cudaGetDevice(&dev));
   ORBIT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
