@@ -123,7 +123,8 @@ class Clocks:
 
 def _make_inputs(rank, n_draws, seed=2024):
     from orbit_b200 import synthetic
-    mets = [synthetic.make_met(seed + 1000 * (rank * 64 + d), NZ, NY, NX, cmfmc_frac=0.3)
+    from orbit_b200.shard import met_draw_seed
+    mets = [synthetic.make_met(met_draw_seed(seed, rank, d), NZ, NY, NX, cmfmc_frac=0.3)
             for d in range(n_draws)]
     spc = [synthetic.make_species(seed + 17 + s, NZ, NY, NX) for s in range(N_SPECIES)]
     sinks = [[s.sink_diag(met) for s in spc] for met in mets]  # [draw][species] (8, N)

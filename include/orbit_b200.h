@@ -205,6 +205,13 @@ int orbit_gmres_solve(orbit_factor_t f, int n_active, const double* e, double dt
                       const double* c_warm, double tol, int maxiter, int restart,
                       double* orbit_out, double* info_out, orbit_stream_t stream);
 
+/* Self-test of the bounded device waits: one chained-solve launch whose first
+ * task waits for a completion count that nothing reaches.  Returns
+ * ORBIT_ERR_TIMEOUT when the wait gave up, the status word was read and every
+ * block left (the context stays usable; the handle's status is reset).  No
+ * reference counterpart (the reference has no device waits). */
+int orbit_selftest_wait_timeout(orbit_factor_t f, orbit_stream_t stream);
+
 /* Transposed periodic-orbit solve (I - M^T) lam0 = s_adj with receptors R
  * (device (n_active, 8, N)); adjoint_out (n_active, 9, N); info_out (n_active, 8)
  * as above.  Replaces solve_orbit_adjoint_one_species

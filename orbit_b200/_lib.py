@@ -66,6 +66,7 @@ EXPORTS = {
     "orbit_factor_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "orbit_chain_apply": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p]),
+    "orbit_selftest_wait_timeout": (C.c_int, [C.c_void_p, C.c_void_p]),
     "orbit_gmres_solve": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_void_p,
                                     C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_void_p]),

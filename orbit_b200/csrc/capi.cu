@@ -48,6 +48,7 @@ int chain_apply_impl(orbit_factor_s* f, int n, int trans, int tau0, int tau1, co
                      double* x_out, const double* forcing, double fscale, int refine, cudaStream_t st);
 int assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T, double* rowsum,
                        cudaStream_t st);
+int chain_wait_selftest(orbit_factor_s* f, const int* d_orbit_ids, cudaStream_t st);
 int mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* Tst,
                       const double* const* rho, double* out_int, double* out_top, cudaStream_t st);
 int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
@@ -562,6 +563,20 @@ int orbit_chain_apply(orbit_factor_t f, int n_active, int trans, int tau0, int t
   std::lock_guard<std::mutex> lk(f->mu);
   return chain_apply_impl(f, n_active, trans, tau0, tau1, x_in, x_out, forcing, fscale, refine,
                           (cudaStream_t)stream);
+}
+
+int orbit_selftest_wait_timeout(orbit_factor_t f, orbit_stream_t stream) {
+  if (!f || f->n_factored < 1) {
+    set_last_error("orbit_selftest_wait_timeout: factor the handle first");
+    return ORBIT_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(f->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int zero = 0;
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->orbit_ids, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+  int rc = chain_wait_selftest(f, f->orbit_ids, st);
+  if (rc == ORBIT_ERR_TIMEOUT) set_last_error("device spin-wait timed out (self-test)");
+  return rc;
 }
 
 int orbit_gmres_solve(orbit_factor_t f, int n_active, const double* e, double dtau, const double* c_warm,

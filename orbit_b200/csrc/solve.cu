@@ -62,6 +62,7 @@ struct ChainDev {
   int B, tau0, tau1, trans;
   int total;
   long long spin_limit;
+  int never_ready;  // self-test: the first task waits for a count nothing reaches
 };
 
 __device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit) {
@@ -398,7 +399,10 @@ __global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(Chain
     // ---- dependencies ----
     if (tid == 0) {
       bool ok = true;
-      if (fwd) {
+      if (D.never_ready && t == 0)
+        ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, 0x7fffffff, D.status, D.spin_limit);
+      if (!ok) {
+      } else if (fwd) {
         if (!subtree)
           for (int q2 = 0; q2 < 2 && ok; ++q2) {
             const int c = D.child[2 * s + q2];
@@ -464,7 +468,7 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
 
 template <typename T>
 int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, int trans, int tau0,
-                   int tau1, const double* E, double escale, cudaStream_t st) {
+                   int tau1, const double* E, double escale, cudaStream_t st, bool never_ready = false) {
   orbit_symbolic_s* sy = f->sym;
   const Symbolic& S = sy->S;
   ChainDev<T> D;
@@ -487,7 +491,8 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.orbit_ids = d_orbit_ids; D.B = B; D.tau0 = tau0; D.tau1 = tau1; D.trans = trans;
   D.set_of = f->set_of; D.n_bins = f->n_bins;
   D.total = (tau1 - tau0) * D.items_per_bin * B;
-  D.spin_limit = 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
+  D.spin_limit = never_ready ? 20000LL : 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
+  D.never_ready = never_ready ? 1 : 0;
   if (D.total <= 0) return ORBIT_OK;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->counters, 0, sizeof(int) * (size_t)f->n_orbits * 16 * S.nsuper, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
@@ -545,6 +550,23 @@ int launch_chain_x(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
 int launch_chain(orbit_factor_s* f, int B, const int* d_orbit_ids, int trans, int tau0, int tau1,
                  const double* E, double escale, cudaStream_t st) {
   return launch_chain_x(f, f->X, B, d_orbit_ids, trans, tau0, tau1, E, escale, st);
+}
+
+// One chain launch whose first task waits for a completion count that is
+// never reached: exercises the bounded wait, the status word and the orderly
+// exit of every CTA.
+int chain_wait_selftest(orbit_factor_s* f, const int* d_orbit_ids, cudaStream_t st) {
+  ORBIT_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(int), st));
+  int rc = f->precision == ORBIT_PREC_FP32
+               ? launch_chain_t<float>(f, f->X, 1, d_orbit_ids, 0, 0, f->n_bins, nullptr, 0.0, st, true)
+               : launch_chain_t<double>(f, f->X, 1, d_orbit_ids, 0, 0, f->n_bins, nullptr, 0.0, st, true);
+  if (rc) return rc;
+  ORBIT_CUDA_TRY(cudaMemcpyAsync(f->h_status, f->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ORBIT_CUDA_TRY(cudaStreamSynchronize(st));
+  const int code = *f->h_status;
+  ORBIT_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(int), st));
+  ORBIT_CUDA_TRY(cudaStreamSynchronize(st));
+  return code;
 }
 
 }  // namespace orbit
