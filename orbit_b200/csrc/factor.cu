@@ -274,43 +274,16 @@ __global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, in
   }
 }
 
-template <typename T>
-__global__ void k_update(FactorDev D, T* fronts, int64_t i0, int p0) {
-  extern __shared__ unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);
-  T* Bs = As + 16 * kLdS;
-  const int4 it = D.items[i0 + blockIdx.x];
-  const int s = it.x, tr = it.y, tc = it.z;
-  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
-  const int nb = min(64, n - p0);
-  const int q0 = p0 + nb;
-  const int r0 = q0 + 64 * tr, c0 = q0 + 64 * tc;
-  const int h = min(64, n + m - r0), w = min(64, n + m - c0);
-  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
-  T acc[4][4];
-  zero_acc(acc);
-  Ld<T> A{F + (int64_t)r0 * ldf + p0, ldf, h, nb, 0, 0};
-  Ld<T> B{F + (int64_t)p0 * ldf + c0, ldf, nb, w, 0, 0};
-  mma_tile(acc, nb, A, B, As, Bs);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int r = ty + 16 * i, c = tx + 16 * j;
-      if (r < h && c < w && (r0 + r < n || c0 + c < n)) F[(int64_t)(r0 + r) * ldf + c0 + c] -= acc[i][j];
-    }
-}
-
 // Register-tiled GEMM of one output tile: C (h x w) -= A (h x K) B (K x w), or
-// C = -A B when `assign`.  Each of 256 threads owns a TM x TN block of outputs;
+// C = -A B when `assign`; outputs with r >= skip_r and c >= skip_c are left
+// untouched.  Each of 256 threads owns a TM x TN block of outputs;
 // the A and B slabs (128 x 16 and 16 x BN) go through shared memory with
 // 16-byte reads of the outer-product operands, and the next slab is prefetched
 // into registers while the current one is multiplied.
 template <typename T, int TM, int TN, int BN>
 __device__ __forceinline__ void gemm_tile(const T* __restrict__ A, int lda, const T* __restrict__ B,
                                           int ldb, T* C, int ldc, int K, int h, int w, bool assign,
-                                          T* As, T* Bs) {
+                                          T* As, T* Bs, int skip_r = 1 << 30, int skip_c = 1 << 30) {
   constexpr int BM = 128, BK = 16;
   constexpr int LDA = BM + 4, LDB = BN + 4;
   constexpr int AL = BM * BK / 256, BL = BK * BN / 256;
@@ -384,7 +357,7 @@ __device__ __forceinline__ void gemm_tile(const T* __restrict__ A, int lda, cons
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
       const int c = tx * TN + j;
-      if (c < w) {
+      if (c < w && !(r >= skip_r && c >= skip_c)) {
         if (assign) C[(int64_t)r * ldc + c] = -acc[i][j];
         else C[(int64_t)r * ldc + c] -= acc[i][j];
       }
@@ -396,23 +369,43 @@ __device__ __forceinline__ void gemm_tile(const T* __restrict__ A, int lda, cons
 // register tile, FP64 as two 128x64 halves.
 template <typename T>
 __device__ __forceinline__ void gemm_128(const T* A, int lda, const T* B, int ldb, T* C, int ldc, int K,
-                                         int h, int w, bool assign, T* smem) {
+                                         int h, int w, bool assign, T* smem, int skip_r = 1 << 30,
+                                         int skip_c = 1 << 30) {
   T* As = smem;
   T* Bs = smem + 16 * (128 + 4);
   if constexpr (sizeof(T) == 4) {
-    gemm_tile<T, 8, 8, 128>(A, lda, B, ldb, C, ldc, K, h, w, assign, As, Bs);
+    gemm_tile<T, 8, 8, 128>(A, lda, B, ldb, C, ldc, K, h, w, assign, As, Bs, skip_r, skip_c);
   } else {
     for (int half = 0; half < 2; ++half) {
       const int cc = 64 * half;
       if (cc >= w) break;
-      gemm_tile<T, 8, 4, 64>(A, lda, B + cc, ldb, C + cc, ldc, K, h, min(64, w - cc), assign, As, Bs);
+      gemm_tile<T, 8, 4, 64>(A, lda, B + cc, ldb, C + cc, ldc, K, h, min(64, w - cc), assign, As, Bs, skip_r,
+                             skip_c - cc);
     }
   }
 }
 
+// Trailing update after pivot block [p0, q0): the 128 x 128 tile (tr, tc) of
+// the rows and columns beyond q0 gets -= L[:, p0:q0] U[p0:q0, :], except its
+// part inside F22 (rows and columns >= n), which the Schur pass updates once.
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_update2(FactorDev D, T* fronts, int64_t i0, int p0) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, tr = it.y, tc = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
+  const int nb = min(64, n - p0);
+  const int q0 = p0 + nb;
+  const int r0 = q0 + 128 * tr, c0 = q0 + 128 * tc;
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  gemm_128<T>(F + (int64_t)r0 * ldf + p0, ldf, F + (int64_t)p0 * ldf + c0, ldf, F + (int64_t)r0 * ldf + c0, ldf,
+              nb, min(128, n + m - r0), min(128, n + m - c0), false, sm, n - r0, n - c0);
+}
+
 // Schur complement of a front: F22 -= L21 U12 (K = n), one 128 x 128 tile per CTA.
 template <typename T>
-__global__ void __launch_bounds__(256) k_schur(FactorDev D, T* fronts, int64_t i0) {
+__global__ void __launch_bounds__(256, 2) k_schur(FactorDev D, T* fronts, int64_t i0) {
   extern __shared__ unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int4 it = D.items[i0 + blockIdx.x];
@@ -447,7 +440,7 @@ __global__ void k_tri_copy(FactorDev D, T* fronts, const T* factors, int64_t i0,
 // kind 0: Pb (m x n) = -L21 inv(L11), tile (tr of m, tc of n), K from 128 tc;
 // kind 1: Qr (n x m) = -inv(U11) U12, tile (tr of n, tc of m), K from 128 tr.
 template <typename T>
-__global__ void __launch_bounds__(256) k_prod2(FactorDev D, const T* fronts, T* factors, int64_t i0, int kind,
+__global__ void __launch_bounds__(256, 2) k_prod2(FactorDev D, const T* fronts, T* factors, int64_t i0, int kind,
                                                int inst_base) {
   extern __shared__ unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
@@ -609,6 +602,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
   { int _r = allow_max_smem((const void*)k_schur<T>); if (_r) return _r; }
   { int _r = allow_max_smem((const void*)k_prod2<T>); if (_r) return _r; }
+  { int _r = allow_max_smem((const void*)k_update2<T>); if (_r) return _r; }
   { int _r = allow_max_smem((const void*)k_diag<T>); if (_r) return _r; }
   { int _r = allow_max_smem((const void*)k_inv<T>); if (_r) return _r; }
   {
@@ -657,7 +651,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
         }
         case FactorLaunch::UPDATE: {
           dim3 g((unsigned)L.items, G);
-          k_update<T><<<g, kThreads, sm_gemm, st>>>(D, cur, L.item_off, L.p0);
+          k_update2<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off, L.p0);
           note_launch();
           break;
         }

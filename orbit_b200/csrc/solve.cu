@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "handles.h"
@@ -93,10 +94,12 @@ __device__ __forceinline__ double dot16(const double2& a, const double* v) {
   return a.x * v[0] + a.y * v[1];
 }
 
-// Per-lane partial of sum_{j0 <= j < j1} a[j] v[j] (a 16-byte aligned at j = 0,
-// v in shared memory, 16-byte aligned); 16-byte loads, four in flight per lane.
-template <typename T>
-__device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0, int j1, int lane) {
+// Per-lane partial of sum_{j0 <= j < j1} a[j] v[j] for a group of G lanes
+// (gl = lane within the group; a 16-byte aligned at j = 0, v in shared memory,
+// 16-byte aligned).  16-byte loads, up to four in flight per lane: the
+// unrolled loop issues its guarded loads before it uses any of them.
+template <typename T, int G = 32>
+__device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0, int j1, int gl) {
   using V = typename Vec16<T>::type;
   constexpr int W = Vec16<T>::w;
   T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
@@ -104,26 +107,61 @@ __device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0
   // vectors, [jb, j1) scalar tail
   const int ja = min((j0 + W - 1) / W * W, j1);
   const int jb = max(ja, j1 / W * W);
-  for (int j = j0 + lane; j < ja; j += 32) acc0 = fma(__ldg(a + j), v[j], acc0);
+  for (int j = j0 + gl; j < ja; j += G) acc0 = fma(__ldg(a + j), v[j], acc0);
   const int nv0 = ja / W, nv1 = jb / W;
   const V* a4 = reinterpret_cast<const V*>(a);
-  int k = nv0 + lane;
-  for (; k + 96 < nv1; k += 128) {
-    const V x0 = __ldg(a4 + k), x1 = __ldg(a4 + k + 32), x2 = __ldg(a4 + k + 64), x3 = __ldg(a4 + k + 96);
+  for (int k = nv0 + gl; k < nv1; k += 4 * G) {
+    const bool b1 = k + G < nv1, b2 = k + 2 * G < nv1, b3 = k + 3 * G < nv1;
+    V x1 = {}, x2 = {}, x3 = {};
+    const V x0 = __ldg(a4 + k);
+    if (b1) x1 = __ldg(a4 + k + G);
+    if (b2) x2 = __ldg(a4 + k + 2 * G);
+    if (b3) x3 = __ldg(a4 + k + 3 * G);
     acc0 += dot16(x0, v + k * W);
-    acc1 += dot16(x1, v + (k + 32) * W);
-    acc2 += dot16(x2, v + (k + 64) * W);
-    acc3 += dot16(x3, v + (k + 96) * W);
+    if (b1) acc1 += dot16(x1, v + (k + G) * W);
+    if (b2) acc2 += dot16(x2, v + (k + 2 * G) * W);
+    if (b3) acc3 += dot16(x3, v + (k + 3 * G) * W);
   }
-  for (; k < nv1; k += 32) acc0 += dot16(__ldg(a4 + k), v + k * W);
-  for (int j = jb + lane; j < j1; j += 32) acc1 = fma(__ldg(a + j), v[j], acc1);
+  for (int j = jb + gl; j < j1; j += G) acc1 = fma(__ldg(a + j), v[j], acc1);
   return (acc0 + acc1) + (acc2 + acc3);
 }
 
-template <typename T>
-__device__ __forceinline__ T dot_row(const T* __restrict__ a, const T* v, int len, int lane) {
-  return warp_sum(dot_seg(a, v, 0, len, lane));
+// Rows [r0, r1) of a row-major block as dot products, G lanes per row, so a
+// warp works on 32 / G rows at once; warps wid, wid + nw, ... of the caller
+// take successive row groups.  partial(g, i, gl) is a lane's share of row i
+// (g is G as a std::integral_constant, for the matching dot_seg stride);
+// store(i, sum) runs on the group's first lane.  The trip count is uniform
+// across the warp (the shuffles are warp-wide).
+template <int G, typename T, typename P, typename S>
+__device__ __forceinline__ void grouped_rows(int r0, int r1, int wid, int nw, P&& partial, S&& store) {
+  constexpr int R = 32 / G;
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1), gr = lane / G;
+  for (int i0 = r0 + wid * R; i0 < r1; i0 += nw * R) {
+    const int i = i0 + gr;
+    T acc = i < r1 ? partial(std::integral_constant<int, G>(), i, gl) : T(0);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (i < r1 && gl == 0) store(i, acc);
+  }
 }
+
+// Lanes per row from the longest row of the range: about four 16-byte
+// vectors per lane, between 4 and 32 lanes.
+template <typename T>
+__device__ __forceinline__ int group_lanes(int maxlen) {
+  const int nv = (maxlen + Vec16<T>::w - 1) / Vec16<T>::w;
+  return nv <= 16 ? 4 : nv <= 32 ? 8 : nv <= 64 ? 16 : 32;
+}
+
+#define ORBIT_GROUPED_ROWS(T, G_, r0, r1, wid, nw, partial, store)           \
+  do {                                                                      \
+    switch (G_) {                                                           \
+      case 4: grouped_rows<4, T>(r0, r1, wid, nw, partial, store); break;   \
+      case 8: grouped_rows<8, T>(r0, r1, wid, nw, partial, store); break;   \
+      case 16: grouped_rows<16, T>(r0, r1, wid, nw, partial, store); break; \
+      default: grouped_rows<32, T>(r0, r1, wid, nw, partial, store); break; \
+    }                                                                       \
+  } while (0)
 
 // Forward step of one supernode (L, or U^T when trans) for output rows
 // [r0, r1): gathers its right-hand side (own entries of Xin, plus forcing) and
@@ -166,14 +204,16 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
   __syncthreads();
   if (!trans) {
     // rows of [SQ; Pb]: row i < n uses the strict lower part (unit diagonal)
-    for (int i = r0 + warp; i < r1; i += kWarps) {
-      const int len = i < n ? i : n;
-      T acc = dot_row(SQ + (int64_t)i * ldn, vec, len, lane);
-      if (lane == 0) {
-        if (i < n) Yo[first + i] = (double)(vec[i] + acc);
-        else Wo[D.woff[s] + (i - n)] = (double)(vec[i] + acc);
-      }
-    }
+    const int64_t woff = D.woff[s];
+    auto partial = [&](auto g, int i, int gl) {
+      return dot_seg<T, decltype(g)::value>(SQ + (int64_t)i * ldn, vec, 0, i < n ? i : n, gl);
+    };
+    auto store = [&](int i, T acc) {
+      if (i < n) Yo[first + i] = (double)(vec[i] + acc);
+      else Wo[woff + (i - n)] = (double)(vec[i] + acc);
+    };
+    const int G = group_lanes<T>(min(r1 - 1, n));
+    ORBIT_GROUPED_ROWS(T, G, r0, r1, warp, kWarps, partial, store);
   } else {
     // columns of [upper(SQ) | Qr]
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
@@ -225,12 +265,14 @@ __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
   __syncthreads();
   if (!trans) {
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
-    for (int i = r0 + warp; i < r1; i += kWarps) {
-      T acc = dot_seg(SQ + (int64_t)i * ldn, vec, i, n, lane);
-      acc += dot_seg(Qr + (int64_t)i * ldm, vec + n0pad, 0, m, lane);
-      acc = warp_sum(acc);
-      if (lane == 0) Xout[first + i] = (double)acc;
-    }
+    auto partial = [&](auto g, int i, int gl) {
+      constexpr int G = decltype(g)::value;
+      return dot_seg<T, G>(SQ + (int64_t)i * ldn, vec, i, n, gl) +
+             dot_seg<T, G>(Qr + (int64_t)i * ldm, vec + n0pad, 0, m, gl);
+    };
+    auto store = [&](int i, T acc) { Xout[first + i] = (double)acc; };
+    const int G = group_lanes<T>(n - r0 + m);
+    ORBIT_GROUPED_ROWS(T, G, r0, r1, warp, kWarps, partial, store);
   } else {
     // columns of [SQ_strict_lower ; Pb] with unit diagonal
     const T* Pb = SQ + (int64_t)n * ldn;
@@ -302,14 +344,15 @@ __device__ void fwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
         else Wo[woff + (i - n)] = (double)(v[i] + acc);
       }
     } else {
-      for (int i = 0; i < n + m; ++i) {
-        const int len = i < n ? i : n;
-        T acc = dot_row(SQ + (int64_t)i * ldn, v, len, lane);
-        if (lane == 0) {
-          if (i < n) Yo[first + i] = (double)(v[i] + acc);
-          else Wo[woff + (i - n)] = (double)(v[i] + acc);
-        }
-      }
+      auto partial = [&](auto g, int i, int gl) {
+        return dot_seg<T, decltype(g)::value>(SQ + (int64_t)i * ldn, v, 0, i < n ? i : n, gl);
+      };
+      auto store = [&](int i, T acc) {
+        if (i < n) Yo[first + i] = (double)(v[i] + acc);
+        else Wo[woff + (i - n)] = (double)(v[i] + acc);
+      };
+      const int G = group_lanes<T>(n);
+      ORBIT_GROUPED_ROWS(T, G, 0, n + m, 0, 1, partial, store);
     }
   } else {
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
@@ -346,12 +389,14 @@ __device__ void bwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
   __syncwarp();
   if (!trans) {
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
-    for (int i = 0; i < n; ++i) {
-      T acc = dot_seg(SQ + (int64_t)i * ldn, v, i, n, lane);
-      acc += dot_seg(Qr + (int64_t)i * ldm, v + n0pad, 0, m, lane);
-      acc = warp_sum(acc);
-      if (lane == 0) Xout[first + i] = (double)acc;
-    }
+    auto partial = [&](auto g, int i, int gl) {
+      constexpr int G = decltype(g)::value;
+      return dot_seg<T, G>(SQ + (int64_t)i * ldn, v, i, n, gl) +
+             dot_seg<T, G>(Qr + (int64_t)i * ldm, v + n0pad, 0, m, gl);
+    };
+    auto store = [&](int i, T acc) { Xout[first + i] = (double)acc; };
+    const int G = group_lanes<T>(n + m);
+    ORBIT_GROUPED_ROWS(T, G, 0, n, 0, 1, partial, store);
   } else {
     const T* Pb = SQ + (int64_t)n * ldn;
     for (int c = lane; c < n; c += 32) {

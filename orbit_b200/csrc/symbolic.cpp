@@ -14,6 +14,7 @@
 #include "symbolic.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <array>
 #include <cmath>
 #include <functional>
@@ -303,13 +304,13 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
         if (S.n[s] <= p0) continue;
         int nb = std::min(kNB, S.n[s] - p0);
         int rest = S.n[s] + S.m[s] - (p0 + nb);
-        int nt = (rest + kTile - 1) / kTile;
+        int nt = (rest + kSchurTile - 1) / kSchurTile;
         const int q0 = p0 + nb;
-        // only tiles touching the pivot rows or columns; the ancestor block
-        // F22 is updated once, after the last pivot block (SCHUR)
+        // only 128-tiles touching the pivot rows or columns; the ancestor
+        // block F22 is updated once, after the last pivot block (SCHUR)
         for (int tr = 0; tr < nt; ++tr)
           for (int tc = 0; tc < nt; ++tc)
-            if (q0 + kTile * tr < S.n[s] || q0 + kTile * tc < S.n[s]) push_item(s, tr, tc, 0);
+            if (q0 + kSchurTile * tr < S.n[s] || q0 + kSchurTile * tc < S.n[s]) push_item(s, tr, tc, 0);
       }
       if (nitems() > off) S.fsched.push_back({FactorLaunch::UPDATE, l, p0, off, nitems() - off});
     }
@@ -403,7 +404,14 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     subw[s] = w;
     sub_node_first[s] = f;
   }
-  const int64_t wmax = std::max<int64_t>(int64_t(4) * chunk_elems, S.fac_nnz / 256);
+  // Off by default: with several rows per warp in the chunked tasks, per-node
+  // chunks beat whole-subtree tasks at every batch size measured (1 to 12
+  // orbits).  ORBIT_B200_SUBTREE_DIV=d enables them below fac_nnz / d work.
+  int64_t wmax = 0;
+  if (const char* e = std::getenv("ORBIT_B200_SUBTREE_DIV")) {
+    const int64_t div = std::atoll(e);
+    wmax = div > 0 ? std::max<int64_t>(1, S.fac_nnz / div) : 0;
+  }
   // role: 0 = chunked node, 1 = subtree root, 2 = inside a subtree
   S.role.assign(ns, 0);
   for (int s = ns - 1; s >= 0; --s) {
