@@ -131,6 +131,7 @@ int build_device_symbolic(orbit_symbolic_s* h) {
   ORBIT_TRY(upload(A, &d.perm, S.perm));
   ORBIT_TRY(upload(A, &d.iperm, S.iperm));
   ORBIT_TRY(upload(A, &d.level, S.level));
+  ORBIT_TRY(upload(A, &d.tc_pack_off, S.tc_pack_off));
   return ORBIT_OK;
 }
 
@@ -409,6 +410,8 @@ int orbit_factor_create_ex(orbit_symbolic_t sym, int n_orbits, int n_sets, int n
   f->front_group = (int)G;
   if ((rc = dalloc(A, reinterpret_cast<unsigned char**>(&f->factors), (size_t)n_inst * S.fac_size * vb))) return fail(rc);
   if ((rc = dalloc(A, reinterpret_cast<unsigned char**>(&f->fronts), (size_t)2 * G * S.front_buf_size * vb))) return fail(rc);
+  if (precision == ORBIT_PREC_FP32 && S.tc_pack_size > 0)
+    if ((rc = dalloc(A, &f->tc_pack, (size_t)G * S.tc_pack_size))) return fail(rc);
   if ((rc = dalloc(A, &f->A_stencil, (size_t)n_inst * 7 * N))) return fail(rc);
   if ((rc = dalloc(A, &f->d_Tptr, (size_t)n_inst))) return fail(rc);
   if ((rc = dalloc(A, &f->d_Dptr, (size_t)n_inst))) return fail(rc);
@@ -512,7 +515,9 @@ int orbit_factor_numeric(orbit_factor_t f, int n_active, const double* const* T_
   ORBIT_CUDA_TRY(cudaMemcpyAsync(f->h_status, f->status, sizeof(int), cudaMemcpyDeviceToHost, st));
   ORBIT_CUDA_TRY(cudaStreamSynchronize(st));
   if (*f->h_status != 0) {
-    set_last_error("zero or non-finite pivot in the numeric factorization");
+    set_last_error(*f->h_status == ORBIT_ERR_TIMEOUT
+                       ? "tensor-core Schur complement: a pipeline wait exceeded its limit"
+                       : "zero or non-finite pivot in the numeric factorization");
     return *f->h_status;
   }
   f->n_factored = n_active;
@@ -530,6 +535,7 @@ int orbit_factor_bytes(orbit_factor_t f, int64_t* numeric_bytes, int64_t* worksp
   if (numeric_bytes) *numeric_bytes = (int64_t)f->n_sets * f->n_bins * S.fac_size * vb;
   if (workspace_bytes)
     *workspace_bytes = (int64_t)2 * f->front_group * S.front_buf_size * vb +
+                       (f->tc_pack ? (int64_t)f->front_group * S.tc_pack_size * 4 : 0) +
                        (int64_t)f->n_sets * f->n_bins * 7 * S.N * 8 +
                        (int64_t)f->n_orbits * (9 + 1 + 8 + 23 + 33) * S.N * 8;
   return ORBIT_OK;

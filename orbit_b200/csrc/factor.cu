@@ -20,11 +20,13 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <type_traits>
 
 #include "common.cuh"
 #include "handles.h"
+#include "tc.cuh"
 
 namespace orbit {
 
@@ -108,6 +110,8 @@ struct FactorDev {
   const int4* items;
   int64_t fac_size, front_buf;
   int group;  // instances per front group
+  const int64_t* tc_pack_off;
+  int64_t tc_pack_stride;  // floats per instance
 };
 
 template <typename T>
@@ -575,6 +579,177 @@ __global__ void k_prod(FactorDev D, const T* fronts, T* factors, int64_t i0, int
   }
 }
 
+// ---- tensor-core Schur complement (fp32 factors) ----
+//
+// F22 -= L21 U12 on the 5th-generation tensor cores with split tf32 operands
+// (x = hi + lo, hi = tf32(x), lo = tf32(x - hi); the product is accumulated as
+// hi*hi + hi*lo + lo*hi in fp32 in tensor memory), which keeps the error of an
+// fp32 GEMM.  k_tc_pack writes each operand tile once, already split and in the
+// swizzled shared-memory layout, so the GEMM moves whole 16 KB hi/lo tile
+// pairs with single bulk copies.
+
+static_assert(tc::kCols == kTcK && tc::kTileFloats == kTcTileFloats, "packed tile geometry");
+
+// One 128 x 16 tile: L21 rows (which 0) or U12 columns (which 1) of node s.
+__global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* fronts, float* pack, int64_t i0) {
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, which = it.y, t = it.z, kb = it.w;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
+  const int mt = (m + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
+  const float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  float* dst = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s] +
+               ((int64_t)which * mt * kt + (int64_t)t * kt + kb) * (2 * tc::kTileFloats);
+  for (int q = threadIdx.x; q < tc::kRows * (tc::kCols / 4); q += blockDim.x) {
+    // A: 4 consecutive threads read one 64-byte row segment; B: consecutive
+    // threads read consecutive columns of one U12 row.
+    const int r = which == 0 ? q >> 2 : q & 127;
+    const int c = which == 0 ? q & 3 : q >> 7;
+    const int row = t * tc::kRows + r;
+    const int k = kb * tc::kCols + c * 4;
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      float x = 0.f;
+      if (row < m && k + u < n)
+        x = which == 0 ? F[(int64_t)(n + row) * ldf + k + u] : F[(int64_t)(k + u) * ldf + n + row];
+      v[u] = x;
+    }
+    float4 hi, lo;
+    hi.x = tc::to_tf32(v[0]); lo.x = tc::to_tf32(v[0] - hi.x);
+    hi.y = tc::to_tf32(v[1]); lo.y = tc::to_tf32(v[1] - hi.y);
+    hi.z = tc::to_tf32(v[2]); lo.z = tc::to_tf32(v[2] - hi.z);
+    hi.w = tc::to_tf32(v[3]); lo.w = tc::to_tf32(v[3] - hi.w);
+    const int o = tc::swz(r, c * 4);
+    *reinterpret_cast<float4*>(dst + o) = hi;
+    *reinterpret_cast<float4*>(dst + tc::kTileFloats + o) = lo;
+  }
+}
+
+constexpr int kTcStages = 3;
+constexpr int kTcStageBytes = 4 * tc::kTileBytes;  // A hi, A lo, B hi, B lo
+constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 512;
+constexpr long long kTcWaitLimit = 1LL << 22;
+
+// One 128 x 128 output tile of F22 per CTA, two CTAs per SM (96 KB ring and
+// 128 TMEM columns each) so that one CTA's epilogue overlaps the other's main
+// loop.  Warp 0 lane 0 streams the k-blocks into a 3-stage ring, warp 1 lane 0
+// issues the MMAs, all four warps read the accumulator back (warp w owns TMEM
+// lanes 32w..32w+31 = tile rows) and stage it through shared memory so that
+// the read-modify-write of F22 goes row by row, coalesced.  Every wait is
+// bounded; on a timeout the CTA lets its copies land, skips the update,
+// raises ORBIT_ERR_TIMEOUT and frees its tensor memory.
+__global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts, const float* pack, int64_t i0,
+                                                     int* status) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t full[kTcStages], empty[kTcStages], done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int failed;
+  const uint32_t raw = tc::smem_u32(smem_raw);
+  unsigned char* sbuf = smem_raw + ((512u - (raw & 511u)) & 511u);
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, tr = it.y, tcol = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
+  const int kt = (n + tc::kCols - 1) / tc::kCols, mt = (m + 127) / 128;
+  const float* pk = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s];
+  const float* pa = pk + (int64_t)tr * kt * (2 * tc::kTileFloats);
+  const float* pb = pk + ((int64_t)mt * kt + (int64_t)tcol * kt) * (2 * tc::kTileFloats);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTcStages; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    tc::mbar_init(&done, 1);
+    failed = 0;
+    tc::fence_barrier_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&tmem_base, 128);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  if (threadIdx.x == 0) {
+    int issued = 0;
+    for (int kb = 0; kb < kt; ++kb) {
+      const int st = kb % kTcStages;
+      if (kb >= kTcStages && !tc::mbar_wait(&empty[st], ((kb / kTcStages) - 1) & 1, kTcWaitLimit)) {
+        failed = 1;
+        break;
+      }
+      unsigned char* sb = sbuf + st * kTcStageBytes;
+      tc::mbar_arrive_expect_tx(&full[st], kTcStageBytes);
+      tc::bulk_g2s(sb, pa + (int64_t)kb * (2 * tc::kTileFloats), 2 * tc::kTileBytes, &full[st]);
+      tc::bulk_g2s(sb + 2 * tc::kTileBytes, pb + (int64_t)kb * (2 * tc::kTileFloats), 2 * tc::kTileBytes,
+                   &full[st]);
+      issued = kb + 1;
+    }
+    // every issued copy has landed before this CTA may finish
+    for (int kb = max(0, issued - kTcStages); kb < issued; ++kb)
+      if (!tc::mbar_wait(&full[kb % kTcStages], (kb / kTcStages) & 1, kTcWaitLimit)) failed = 1;
+  } else if (threadIdx.x == 32) {
+    const uint32_t idesc = tc::idesc_tf32(128, 128);
+    for (int kb = 0; kb < kt; ++kb) {
+      const int st = kb % kTcStages;
+      if (!tc::mbar_wait(&full[st], (kb / kTcStages) & 1, kTcWaitLimit)) {
+        failed = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t a = tc::smem_u32(sbuf + st * kTcStageBytes);
+      const uint32_t ahi = a, alo = a + tc::kTileBytes, bhi = a + 2 * tc::kTileBytes, blo = a + 3 * tc::kTileBytes;
+#pragma unroll
+      for (int kk = 0; kk < tc::kCols / 8; ++kk) {
+        const uint32_t o = kk * 32;  // 8 tf32 along K inside the 64-byte swizzled row
+        tc::mma_tf32(tmem, tc::sw64_desc(ahi + o), tc::sw64_desc(bhi + o), idesc, (kb | kk) != 0);
+        tc::mma_tf32(tmem, tc::sw64_desc(ahi + o), tc::sw64_desc(blo + o), idesc, 1);
+        tc::mma_tf32(tmem, tc::sw64_desc(alo + o), tc::sw64_desc(bhi + o), idesc, 1);
+      }
+      tc::mma_commit(&empty[st]);
+    }
+    tc::mma_commit(&done);
+  }
+  const bool ok = tc::mbar_wait(&done, 0, kTcWaitLimit);
+  tc::fence_after_sync();
+  const int good = __syncthreads_and(ok ? 1 : 0) && !failed;
+  if (good) {
+    // the ring is idle now: each warp transposes its 32 x 32 accumulator
+    // blocks through a private padded buffer
+    float* sw = reinterpret_cast<float*>(sbuf) + warp * 32 * 33;
+    const int rows = min(32, m - tr * tc::kRows - warp * 32);
+    const int cols = min(128, m - tcol * 128);
+    float* C = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s] +
+               (int64_t)(n + tr * tc::kRows + warp * 32) * ldf + n + tcol * 128;
+    for (int cc = 0; cc < 4 && cc * 32 < cols; ++cc) {
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) sw[lane * 33 + j] = v[j];
+      __syncwarp();
+      const int col = cc * 32 + lane;
+      if (col < cols) {
+        for (int r0 = 0; r0 < rows; r0 += 8) {
+          float c[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (r0 + u < rows) c[u] = C[(int64_t)(r0 + u) * ldf + col];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (r0 + u < rows) C[(int64_t)(r0 + u) * ldf + col] = c[u] - sw[(r0 + u) * 33 + lane];
+        }
+      }
+      __syncwarp();
+    }
+  } else if (threadIdx.x == 0) {
+    raise_status(status, ORBIT_ERR_TIMEOUT);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 1) tc::tmem_dealloc(tmem, 128);
+}
+
 inline int clamp_grid(int64_t blocks) {
   if (blocks < 1) return 1;
   if (blocks > (1 << 20)) return 1 << 20;
@@ -593,6 +768,8 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   D.fac_size = S.fac_size;
   D.front_buf = S.front_buf_size;
   D.group = f->front_group;
+  D.tc_pack_off = sy->d.tc_pack_off;
+  D.tc_pack_stride = S.tc_pack_size;
   T* factors = reinterpret_cast<T*>(f->factors);
   T* fronts = reinterpret_cast<T*>(f->fronts);
   const int n_inst = n_active * f->n_bins;
@@ -601,6 +778,12 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   const size_t sm_diag = 3 * 64 * kLdS * sizeof(T);
   const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
   { int _r = allow_max_smem((const void*)k_schur<T>); if (_r) return _r; }
+  bool use_tc = false;
+  if constexpr (std::is_same<T, float>::value) {
+    const char* e = std::getenv("ORBIT_B200_TC");
+    use_tc = f->tc_pack != nullptr && !(e && e[0] == '0');
+    if (use_tc) { int _r = allow_max_smem((const void*)k_schur_tc); if (_r) return _r; }
+  }
   { int _r = allow_max_smem((const void*)k_prod2<T>); if (_r) return _r; }
   { int _r = allow_max_smem((const void*)k_update2<T>); if (_r) return _r; }
   { int _r = allow_max_smem((const void*)k_diag<T>); if (_r) return _r; }
@@ -655,10 +838,30 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
           note_launch();
           break;
         }
+        case FactorLaunch::TC_PACK: {
+          if constexpr (std::is_same<T, float>::value) {
+            if (use_tc) {
+              dim3 g((unsigned)L.items, G);
+              k_tc_pack<<<g, 256, 0, st>>>(D, cur, f->tc_pack, L.item_off);
+              note_launch();
+            }
+          }
+          break;
+        }
         case FactorLaunch::SCHUR: {
-          dim3 g((unsigned)L.items, G);
-          k_schur<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off);
-          note_launch();
+          const int64_t n_cc = use_tc ? L.p0 : L.items;
+          if (n_cc > 0) {
+            dim3 g((unsigned)n_cc, G);
+            k_schur<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off);
+            note_launch();
+          }
+          if constexpr (std::is_same<T, float>::value) {
+            if (use_tc && L.items > L.p0) {
+              dim3 g((unsigned)(L.items - L.p0), G);
+              k_schur_tc<<<g, 128, kTcSmem, st>>>(D, cur, f->tc_pack, L.item_off + L.p0, f->status);
+              note_launch();
+            }
+          }
           break;
         }
         case FactorLaunch::INV: {

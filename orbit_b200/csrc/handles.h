@@ -24,6 +24,7 @@ struct DevSym {
   int32_t *nchunk_fwd = nullptr, *nchunk_bwd = nullptr, *nchunk_fwdT = nullptr, *nchunk_bwdT = nullptr;
   int32_t *perm = nullptr, *iperm = nullptr;
   int32_t *level = nullptr;
+  int64_t *tc_pack_off = nullptr;
 };
 
 struct orbit_symbolic_s {
@@ -51,6 +52,9 @@ struct orbit_factor_s {
   // front workspace: 2 parity buffers x group instances x front_buf_size
   void* fronts = nullptr;
   int front_group = 1;
+  // fp32 factors: tf32 hi/lo operand packs of the tensor-core Schur
+  // complements, front_group instances x tc_pack_size floats
+  float* tc_pack = nullptr;
   // FP64 copies of A = I + dtau (T + diag(sink)) as 7-point stencils, per instance
   double* A_stencil = nullptr;
   // device pointer tables (per instance) used by the scatter kernel

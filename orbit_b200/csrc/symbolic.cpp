@@ -262,6 +262,10 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     }
 
   // ---- factorization schedule ----
+  S.tc_min_n = 96;
+  if (const char* e = std::getenv("ORBIT_B200_TC_MIN_N")) S.tc_min_n = std::max(1, std::atoi(e));
+  S.tc_pack_off.assign(ns, -1);
+  S.tc_pack_size = 0;
   auto push_item = [&](int a, int b, int c, int d) {
     S.fitems.push_back(a); S.fitems.push_back(b); S.fitems.push_back(c); S.fitems.push_back(d);
   };
@@ -315,15 +319,36 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
       if (nitems() > off) S.fsched.push_back({FactorLaunch::UPDATE, l, p0, off, nitems() - off});
     }
     {
-      int64_t off = nitems();
+      // Schur complements: nodes below the tensor-core threshold first (their
+      // item count goes in p0), then the tensor-core nodes, whose operands a
+      // TC_PACK launch packs first.
+      std::vector<int> small, big;
       for (int s : sups) {
-        const int mm = S.m[s];
-        if (mm == 0 || S.n[s] == 0) continue;
-        const int nt = (mm + kSchurTile - 1) / kSchurTile;
-        for (int tr = 0; tr < nt; ++tr)
-          for (int tc = 0; tc < nt; ++tc) push_item(s, tr, tc, 0);
+        if (S.m[s] == 0 || S.n[s] == 0) continue;
+        (S.n[s] >= S.tc_min_n ? big : small).push_back(s);
       }
-      if (nitems() > off) S.fsched.push_back({FactorLaunch::SCHUR, l, 0, off, nitems() - off});
+      int64_t pack = 0;
+      int64_t off = nitems();
+      for (int s : big) {
+        const int mt = (S.m[s] + kSchurTile - 1) / kSchurTile, kt = (S.n[s] + kTcK - 1) / kTcK;
+        S.tc_pack_off[s] = pack;
+        pack += int64_t(2) * mt * kt * 2 * kTcTileFloats;
+        for (int which = 0; which < 2; ++which)
+          for (int t = 0; t < mt; ++t)
+            for (int k = 0; k < kt; ++k) push_item(s, which, t, k);
+      }
+      S.tc_pack_size = std::max(S.tc_pack_size, pack);
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::TC_PACK, l, 0, off, nitems() - off});
+      off = nitems();
+      int nsmall = 0;
+      for (int pass = 0; pass < 2; ++pass)
+        for (int s : pass == 0 ? small : big) {
+          const int nt = (S.m[s] + kSchurTile - 1) / kSchurTile;
+          for (int tr = 0; tr < nt; ++tr)
+            for (int tc = 0; tc < nt; ++tc) push_item(s, tr, tc, 0);
+          if (pass == 0) nsmall += nt * nt;
+        }
+      if (nitems() > off) S.fsched.push_back({FactorLaunch::SCHUR, l, nsmall, off, nitems() - off});
     }
     // blocked triangular inverses: step t fills block row t of Linv and block column t of Uinv
     int tmax = (nmax + kNB - 1) / kNB;
