@@ -98,7 +98,7 @@ int orbit_symbolic_perm(orbit_symbolic_t sym, int32_t* perm_host);
  * analysis stores it) for inspection and host-side checks; dst may be NULL to
  * query *count.  Names: perm, iperm, first, n, m, parent, level, child, uoff,
  * uidx, rel, ldn, ldm, ldf, fac_off, front_off, level_front_size,
- * ent_level_off, ent_pos, ent_src, woff, sitems, phase_off, phase_offT,
+ * ent_level_off, ent_pos, ent_src, ginv, ginv_off, woff, sitems, phase_off, phase_offT,
  * nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT.  No reference counterpart
  * (UMFPACK's symbolic object is opaque); it exists so the structure can be
  * verified on a host without a GPU.  The analysis itself never touches the

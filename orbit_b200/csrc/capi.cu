@@ -132,6 +132,8 @@ int build_device_symbolic(orbit_symbolic_s* h) {
   ORBIT_TRY(upload(A, &d.iperm, S.iperm));
   ORBIT_TRY(upload(A, &d.level, S.level));
   ORBIT_TRY(upload(A, &d.tc_pack_off, S.tc_pack_off));
+  ORBIT_TRY(upload(A, &d.ginv, S.ginv));
+  ORBIT_TRY(upload(A, &d.ginv_off, S.ginv_off));
   return ORBIT_OK;
 }
 
@@ -265,6 +267,7 @@ int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int6
   ORBIT_ARR("ldm", ldm) ORBIT_ARR("ldf", ldf) ORBIT_ARR("fac_off", fac_off)
   ORBIT_ARR("front_off", front_off) ORBIT_ARR("level_front_size", level_front_size)
   ORBIT_ARR("ent_level_off", ent_level_off) ORBIT_ARR("ent_pos", ent_pos) ORBIT_ARR("ent_src", ent_src)
+  ORBIT_ARR("ginv", ginv) ORBIT_ARR("ginv_off", ginv_off)
   ORBIT_ARR("woff", woff) ORBIT_ARR("sitems", sitems) ORBIT_ARR("phase_off", phase_off)
   ORBIT_ARR("phase_offT", phase_offT) ORBIT_ARR("nchunk_fwd", nchunk_fwd)
   ORBIT_ARR("nchunk_bwd", nchunk_bwd) ORBIT_ARR("nchunk_fwdT", nchunk_fwdT)
@@ -274,7 +277,7 @@ int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int6
     bool known = false;
     for (const char* k : {"perm", "iperm", "first", "n", "m", "parent", "level", "child", "uoff", "uidx",
                           "rel", "ldn", "ldm", "ldf", "fac_off", "front_off", "level_front_size",
-                          "ent_level_off", "ent_pos", "ent_src", "woff", "phase_off", "phase_offT",
+                          "ent_level_off", "ent_pos", "ent_src", "ginv", "ginv_off", "woff", "phase_off", "phase_offT",
                           "nchunk_fwd", "nchunk_bwd", "nchunk_fwdT", "nchunk_bwdT"})
       known = known || nm == k;
     if (!known) {

@@ -105,7 +105,9 @@ __device__ __forceinline__ void zero_acc(T (&acc)[4][4]) {
 }
 
 struct FactorDev {
-  const int32_t *n, *m, *parent, *rel, *ldn, *ldm, *ldf;
+  const int32_t *n, *m, *parent, *child, *rel, *ldn, *ldm, *ldf;
+  const int32_t* ginv;
+  const int64_t* ginv_off;
   const int64_t *uoff, *fac_off, *front_off;
   const int4* items;
   int64_t fac_size, front_buf;
@@ -114,13 +116,6 @@ struct FactorDev {
   int64_t tc_pack_stride;  // floats per instance
 };
 
-template <typename T>
-__global__ void k_zero(T* fronts, int64_t count, int64_t stride) {
-  T* f = fronts + (int64_t)blockIdx.y * stride;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < count;
-       e += (int64_t)gridDim.x * blockDim.x)
-    f[e] = T(0);
-}
 
 template <typename T>
 __global__ void k_scatter(T* fronts, int64_t stride, const int64_t* ent_pos, const int32_t* ent_src,
@@ -137,7 +132,7 @@ __global__ void k_scatter(T* fronts, int64_t stride, const int64_t* ent_pos, con
     int64_t cell = src - (int64_t)d * N;
     double t = Tv[src];
     double val = d == 0 ? 1.0 + dtau * (t + (Dv ? Dv[cell] : 0.0)) : dtau * t;
-    f[ent_pos[e0 + e]] = (T)val;
+    f[ent_pos[e0 + e]] += (T)val;
   }
 }
 
@@ -155,20 +150,52 @@ __global__ void k_copy_A(double* A, const double* const* Tp, const double* const
   }
 }
 
+// Front assembly by gather: row i of the front of s is the sum of the two
+// children's Schur-complement rows mapped through the inverse extend-add maps
+// (zero where no child contributes), written once together with its padding
+// columns.  The stencil entries are added afterwards (k_scatter).  One warp
+// per row: the stores are contiguous and the children's rows are read in
+// increasing column order.
 template <typename T>
-__global__ void k_extend(FactorDev D, T* fr_par, const T* fr_child, int64_t i0) {
+__global__ void __launch_bounds__(256) k_assemble(FactorDev D, T* fr, const T* fr_child, int64_t i0) {
+  extern __shared__ int32_t sinv[];  // 2 x (n + m)
   const int4 it = D.items[i0 + blockIdx.x];
-  const int c = it.x, rb = it.y;
-  const int p = D.parent[c];
-  const int nc = D.n[c], mc = D.m[c];
-  const int ldc = D.ldf[c], ldp = D.ldf[p];
-  const T* S = fr_child + (int64_t)blockIdx.y * D.front_buf + D.front_off[c] + (int64_t)nc * ldc + nc;
-  T* F = fr_par + (int64_t)blockIdx.y * D.front_buf + D.front_off[p];
-  const int32_t* rel = D.rel + D.uoff[c];
+  const int s = it.x, r0 = it.y, r1 = it.z;
+  const int n = D.n[s], m = D.m[s], w = n + m, ldf = D.ldf[s];
+  const int32_t* gi = D.ginv + D.ginv_off[s];
+  for (int j = threadIdx.x; j < 2 * w; j += blockDim.x) sinv[j] = gi[j];
+  __syncthreads();
+  T* F = fr + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  const T* Sc[2] = {nullptr, nullptr};
+  int ldc[2] = {0, 0};
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int c = D.child[2 * s + q];
+    if (c >= 0) {
+      ldc[q] = D.ldf[c];
+      Sc[q] = fr_child + (int64_t)blockIdx.y * D.front_buf + D.front_off[c] + (int64_t)D.n[c] * ldc[q] + D.n[c];
+    }
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = rb * 32 + warp; i < min(rb * 32 + 32, mc); i += kThreads / 32) {
-    const int64_t prow = (int64_t)rel[i] * ldp;
-    for (int j = lane; j < mc; j += 32) F[prow + rel[j]] += S[(int64_t)i * ldc + j];
+  for (int i = r0 + warp; i < r1; i += blockDim.x / 32) {
+    const int u0 = sinv[i], u1 = sinv[w + i];
+    const T* s0 = u0 >= 0 ? Sc[0] + (int64_t)u0 * ldc[0] : nullptr;
+    const T* s1 = u1 >= 0 ? Sc[1] + (int64_t)u1 * ldc[1] : nullptr;
+    T* row = F + (int64_t)i * ldf;
+    for (int j = lane; j < ldf; j += 32) {
+      T v = T(0);
+      if (j < w) {
+        if (s0) {
+          const int v0 = sinv[j];
+          if (v0 >= 0) v += s0[v0];
+        }
+        if (s1) {
+          const int v1 = sinv[w + j];
+          if (v1 >= 0) v += s1[v1];
+        }
+      }
+      row[j] = v;
+    }
   }
 }
 
@@ -761,7 +788,8 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   orbit_symbolic_s* sy = f->sym;
   const Symbolic& S = sy->S;
   FactorDev D;
-  D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent; D.rel = sy->d.rel;
+  D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent; D.child = sy->d.child; D.rel = sy->d.rel;
+  D.ginv = sy->d.ginv; D.ginv_off = sy->d.ginv_off;
   D.ldn = sy->d.ldn; D.ldm = sy->d.ldm; D.ldf = sy->d.ldf;
   D.uoff = sy->d.uoff; D.fac_off = sy->d.fac_off; D.front_off = sy->d.front_off;
   D.items = sy->d.fitems;
@@ -801,9 +829,9 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
       T* chl = fronts + (int64_t)((L.level + 1) & 1) * f->front_group * S.front_buf_size;
       if (L.items <= 0) continue;
       switch (L.kind) {
-        case FactorLaunch::ZERO: {
-          dim3 g(clamp_grid((L.items + 255) / 256), G);
-          k_zero<T><<<g, 256, 0, st>>>(cur, L.items, S.front_buf_size);
+        case FactorLaunch::ASSEMBLE: {
+          dim3 g((unsigned)L.items, G);
+          k_assemble<T><<<g, 256, sizeof(int32_t) * 2 * S.max_front, st>>>(D, cur, chl, L.item_off);
           note_launch();
           break;
         }
@@ -811,12 +839,6 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
           dim3 g(clamp_grid((L.items + 255) / 256), G);
           k_scatter<T><<<g, 256, 0, st>>>(cur, S.front_buf_size, sy->d.ent_pos, sy->d.ent_src,
                                           L.item_off, L.items, f->d_Tptr, f->d_Dptr, base, S.N, dtau);
-          note_launch();
-          break;
-        }
-        case FactorLaunch::EXTEND: {
-          dim3 g((unsigned)L.items, G);
-          k_extend<T><<<g, kThreads, 0, st>>>(D, cur, chl, L.item_off);
           note_launch();
           break;
         }

@@ -25,6 +25,8 @@ struct DevSym {
   int32_t *perm = nullptr, *iperm = nullptr;
   int32_t *level = nullptr;
   int64_t *tc_pack_off = nullptr;
+  int32_t *ginv = nullptr;
+  int64_t *ginv_off = nullptr;
 };
 
 struct orbit_symbolic_s {

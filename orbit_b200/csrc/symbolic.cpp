@@ -181,6 +181,17 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
       S.rel[S.uoff[s] + q] = pos;
     }
   }
+  S.ginv_off.assign(ns + 1, 0);
+  for (int s = 0; s < ns; ++s) S.ginv_off[s + 1] = S.ginv_off[s] + 2 * int64_t(S.n[s] + S.m[s]);
+  S.ginv.assign(S.ginv_off[ns], -1);
+  for (int s = 0; s < ns; ++s) {
+    const int w = S.n[s] + S.m[s];
+    for (int q = 0; q < 2; ++q) {
+      const int c = S.child[2 * s + q];
+      if (c < 0) continue;
+      for (int u = 0; u < S.m[c]; ++u) S.ginv[S.ginv_off[s] + int64_t(q) * w + S.rel[S.uoff[c] + u]] = u;
+    }
+  }
 
   // ---- levels, storage ----
   int maxd = 0;
@@ -272,19 +283,20 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
   auto nitems = [&]() { return int64_t(S.fitems.size() / 4); };
   for (int l = S.nlevels - 1; l >= 0; --l) {
     const auto& sups = S.level_sups[l];
-    S.fsched.push_back({FactorLaunch::ZERO, l, 0, 0, S.level_front_size[l]});
-    S.fsched.push_back({FactorLaunch::SCATTER, l, 0, S.ent_level_off[l],
-                        S.ent_level_off[l + 1] - S.ent_level_off[l]});
-    for (int slot = 0; slot < 2; ++slot) {
+    {
+      // every front row written once: the children's Schur complements
+      // gathered through the inverse maps, zeros elsewhere; then the stencil
+      // entries are added (SCATTER)
       int64_t off = nitems();
       for (int s : sups) {
-        int c = S.child[2 * s + slot];
-        if (c < 0) continue;
-        int rows = S.m[c];
-        for (int rb = 0; rb * 32 < rows; ++rb) push_item(c, rb, 0, 0);
+        const int w = S.n[s] + S.m[s];
+        const int rows = std::max(1, std::min(32, 8192 / std::max(1, int(S.ldf[s]))));
+        for (int r0 = 0; r0 < w; r0 += rows) push_item(s, r0, std::min(w, r0 + rows), 0);
       }
-      if (nitems() > off) S.fsched.push_back({FactorLaunch::EXTEND, l, slot, off, nitems() - off});
+      S.fsched.push_back({FactorLaunch::ASSEMBLE, l, 0, off, nitems() - off});
     }
+    S.fsched.push_back({FactorLaunch::SCATTER, l, 0, S.ent_level_off[l],
+                        S.ent_level_off[l + 1] - S.ent_level_off[l]});
     int nmax = 0;
     for (int s : sups) nmax = std::max(nmax, S.n[s]);
     for (int p0 = 0; p0 < nmax; p0 += kNB) {

@@ -31,7 +31,7 @@ inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 // One kernel launch of the numeric factorization schedule.
 struct FactorLaunch {
-  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU, TC_PACK } kind;
+  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU, TC_PACK, ASSEMBLE } kind;
   int level;
   int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV); SCHUR: leading items of CUDA-core nodes
   int64_t item_off;  // offset into the item array (int4 units)
@@ -62,6 +62,10 @@ struct Symbolic {
   std::vector<int64_t> level_front_size;  // elements per instance per level
   int64_t front_buf_size = 0;             // max over levels of level_front_size
   std::vector<int64_t> woff;              // update-vector offset per supernode
+  // inverse extend-add maps: for supernode s, 2 x (n+m) ints at ginv_off[s];
+  // entry [q][i] is the update index u of child q with rel_c[u] == i, or -1
+  std::vector<int32_t> ginv;
+  std::vector<int64_t> ginv_off;
   int64_t w_size = 0;
   // per level: supernodes of that level
   std::vector<std::vector<int32_t>> level_sups;

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _lib
 
-_INT64_ARRAYS = {"uoff", "fac_off", "front_off", "level_front_size", "ent_level_off", "ent_pos", "woff"}
+_INT64_ARRAYS = {"ginv_off", "uoff", "fac_off", "front_off", "level_front_size", "ent_level_off", "ent_pos", "woff"}
 
 INFO_KEYS = ("N", "nsuper", "nlevels", "factor_nnz", "factor_elems", "front_elems", "max_front",
              "factor_flops", "solve_items_per_bin", "update_len", "leaf_cells", "max_nm",

@@ -46,7 +46,7 @@ def _matrix(nz, ny, nx, seed=3):
 def _replay(sym, stencil):
     a = {k: sym.array(k) for k in ("perm", "first", "n", "m", "parent", "level", "child", "uoff",
                                    "uidx", "rel", "ldf", "front_off", "level_front_size",
-                                   "ent_level_off", "ent_pos", "ent_src")}
+                                   "ent_level_off", "ent_pos", "ent_src", "ginv", "ginv_off")}
     ns = len(a["n"])
     nlev = int(a["level"].max()) + 1
     flat = stencil.reshape(-1)
@@ -58,11 +58,16 @@ def _replay(sym, stencil):
         for s in np.nonzero(a["level"] == lev)[0]:
             n, m, ld = int(a["n"][s]), int(a["m"][s]), int(a["ldf"][s])
             F = buf[a["front_off"][s]:a["front_off"][s] + (n + m) * ld].reshape(n + m, ld)[:, :n + m].copy()
-            for c in a["child"][2 * s:2 * s + 2]:
+            # gather form of the extend-add (as the assembly kernel does it):
+            # F[i, j] += S_c[inv_c[i], inv_c[j]] wherever both are mapped
+            w = n + m
+            inv = a["ginv"][a["ginv_off"][s]:a["ginv_off"][s] + 2 * w].reshape(2, w)
+            for q, c in enumerate(a["child"][2 * s:2 * s + 2]):
                 if c < 0:
                     continue
-                rel = a["rel"][a["uoff"][c]:a["uoff"][c + 1]]
-                F[np.ix_(rel, rel)] += fronts.pop(c)
+                Sc = fronts.pop(c)
+                rows = np.nonzero(inv[q] >= 0)[0]
+                F[np.ix_(rows, rows)] += Sc[np.ix_(inv[q][rows], inv[q][rows])]
             F11, F12, F21, F22 = F[:n, :n], F[:n, n:], F[n:, :n], F[n:, n:]
             Lw = np.eye(n)
             U = F11.copy()
@@ -130,6 +135,17 @@ def test_structure(shape, leaf):
         assert np.all(np.diff(u) > 0)
         assert np.all(u >= first[s] + n[s])  # only later (ancestor) unknowns
     assert sym.lunz == int((n.astype(np.int64) ** 2 + 2 * n.astype(np.int64) * m).sum())
+    # inverse extend-add maps: ginv[s][q][rel_c[u]] == u for child q, -1 elsewhere
+    child, rel, ginv, goff = sym.array("child"), sym.array("rel"), sym.array("ginv"), sym.array("ginv_off")
+    for s in range(len(n)):
+        w = int(n[s] + m[s])
+        inv = ginv[goff[s]:goff[s] + 2 * w].reshape(2, w)
+        for q in range(2):
+            c = child[2 * s + q]
+            expect = np.full(w, -1)
+            if c >= 0:
+                expect[rel[uoff[c]:uoff[c + 1]]] = np.arange(uoff[c + 1] - uoff[c])
+            assert np.array_equal(inv[q], expect)
 
 
 @pytest.mark.parametrize("shape,leaf", [((3, 4, 5), 4), ((5, 7, 6), 16), ((4, 9, 11), 8)])
