@@ -19,6 +19,7 @@
 // complement F22 - L21 U12 stays in the front for the parent.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -114,7 +115,13 @@ struct FactorDev {
   int group;  // instances per front group
   const int64_t* tc_pack_off;
   int64_t tc_pack_stride;  // floats per instance
+  int tc_min_n;            // nodes with n >= tc_min_n and m > 0 take the tensor-core pipeline
 };
+
+// True for the supernodes whose factorization the tensor-core pipeline
+// completes: their pivot LU stays inside F11 and the triangle copies and
+// CUDA-core panel products skip them.
+__device__ __forceinline__ bool tc_node(const FactorDev& D, int n, int m) { return m > 0 && n >= D.tc_min_n; }
 
 
 template <typename T>
@@ -273,13 +280,15 @@ __global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, in
   const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s];
   const int nb = min(64, n - p0);
   const int q0 = p0 + nb;
+  const int lim = tc_node(D, n, m) ? n : n + m;  // last row / column the panels reach
+  if (q0 + 64 * ch >= lim) return;
   T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   const T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
   T acc[4][4];
   zero_acc(acc);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   if (kind == 0) {
-    const int c0 = q0 + 64 * ch, w = min(64, n + m - c0);
+    const int c0 = q0 + 64 * ch, w = min(64, lim - c0);
     Ld<T> A{SQ + (int64_t)p0 * ldn + p0, ldn, nb, nb, 1, 0};
     Ld<T> B{F + (int64_t)p0 * ldf + c0, ldf, nb, w, 0, 0};
     mma_tile(acc, nb, A, B, As, Bs);
@@ -291,7 +300,7 @@ __global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, in
         if (r < nb && c < w) F[(int64_t)(p0 + r) * ldf + c0 + c] = acc[i][j];
       }
   } else {
-    const int r0 = q0 + 64 * ch, h = min(64, n + m - r0);
+    const int r0 = q0 + 64 * ch, h = min(64, lim - r0);
     Ld<T> A{F + (int64_t)r0 * ldf + p0, ldf, h, nb, 0, 0};
     Ld<T> B{SQ + (int64_t)p0 * ldn + p0, ldn, nb, nb, 2, 0};
     mma_tile(acc, nb, A, B, As, Bs);
@@ -429,9 +438,11 @@ __global__ void __launch_bounds__(256, 2) k_update2(FactorDev D, T* fronts, int6
   const int nb = min(64, n - p0);
   const int q0 = p0 + nb;
   const int r0 = q0 + 128 * tr, c0 = q0 + 128 * tc;
+  const int lim = tc_node(D, n, m) ? n : n + m;
+  if (r0 >= lim || c0 >= lim) return;
   T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   gemm_128<T>(F + (int64_t)r0 * ldf + p0, ldf, F + (int64_t)p0 * ldf + c0, ldf, F + (int64_t)r0 * ldf + c0, ldf,
-              nb, min(128, n + m - r0), min(128, n + m - c0), false, sm, n - r0, n - c0);
+              nb, min(128, lim - r0), min(128, lim - c0), false, sm, n - r0, n - c0);
 }
 
 // Schur complement of a front: F22 -= L21 U12 (K = n), one 128 x 128 tile per CTA.
@@ -456,6 +467,7 @@ __global__ void k_tri_copy(FactorDev D, T* fronts, const T* factors, int64_t i0,
   const int4 it = D.items[i0 + blockIdx.x];
   const int s = it.x, rb = it.y;
   const int n = D.n[s], ldf = D.ldf[s], ldn = D.ldn[s];
+  if (tc_node(D, n, D.m[s])) return;
   T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   const T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
   for (int r = rb * 16 + (threadIdx.x >> 5); r < min(n, rb * 16 + 16); r += 8)
@@ -478,6 +490,7 @@ __global__ void __launch_bounds__(256, 2) k_prod2(FactorDev D, const T* fronts, 
   const int4 it = D.items[i0 + blockIdx.x];
   const int s = it.x, tr = it.y, tc = it.z;
   const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s], ldm = D.ldm[s];
+  if (tc_node(D, n, m)) return;
   const T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
   const int r0 = 128 * tr, c0 = 128 * tc;
@@ -557,88 +570,72 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
   }
 }
 
-template <typename T>
-__global__ void k_prod(FactorDev D, const T* fronts, T* factors, int64_t i0, int inst_base) {
-  extern __shared__ unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);
-  T* Bs = As + 16 * kLdS;
-  const int4 it = D.items[i0 + blockIdx.x];
-  const int s = it.x, kind = it.y, a = it.z, b = it.w;
-  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s], ldm = D.ldm[s];
-  const T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
-  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
-  const int nbk = (n + 63) / 64;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  T acc[4][4];
-  zero_acc(acc);
-  if (kind == 0) {
-    const int r0 = 64 * a, h = min(64, m - r0), c0 = 64 * b, w = min(64, n - c0);
-    for (int kb = b; kb < nbk; ++kb) {
-      const int kw = min(64, n - 64 * kb);
-      Ld<T> A{F + (int64_t)(n + r0) * ldf + 64 * kb, ldf, h, kw, 0, 0};
-      Ld<T> B{SQ + (int64_t)(64 * kb) * ldn + c0, ldn, kw, w, kb == b ? 1 : 0, 0};
-      mma_tile(acc, kw, A, B, As, Bs);
-    }
-    T* Pb = SQ + (int64_t)n * ldn;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int r = ty + 16 * i, c = tx + 16 * j;
-        if (r < h && c < w) Pb[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
-      }
-  } else {
-    const int r0 = 64 * a, h = min(64, n - r0), c0 = 64 * b, w = min(64, m - c0);
-    for (int kb = a; kb < nbk; ++kb) {
-      const int kw = min(64, n - 64 * kb);
-      Ld<T> A{SQ + (int64_t)r0 * ldn + 64 * kb, ldn, h, kw, kb == a ? 2 : 0, 0};
-      Ld<T> B{F + (int64_t)(64 * kb) * ldf + n + c0, ldf, kw, w, 0, 0};
-      mma_tile(acc, kw, A, B, As, Bs);
-    }
-    T* Qr = SQ + (int64_t)(n + m) * ldn;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int r = ty + 16 * i, c = tx + 16 * j;
-        if (r < h && c < w) Qr[(int64_t)(r0 + r) * ldm + c0 + c] = -acc[i][j];
-      }
-  }
-}
-
-// ---- tensor-core Schur complement (fp32 factors) ----
+// ---- tensor-core pipeline (fp32 factors) ----
 //
-// F22 -= L21 U12 on the 5th-generation tensor cores with split tf32 operands
-// (x = hi + lo, hi = tf32(x), lo = tf32(x - hi); the product is accumulated as
+// For the large supernodes the pivot LU stays inside F11, the inverses
+// inv(L11), inv(U11) are formed as for every node, and then
+//   X  = inv(U11) inv(L11)      (= inv(F11))
+//   Pb = -F21 X                 (= -L21 inv(L11))
+//   Qr = -X F12                 (= -inv(U11) U12)
+//   F22 += Pb F12               (= F22 - L21 U12)
+// run on the 5th-generation tensor cores with split tf32 operands
+// (x = hi + lo, hi = tf32(x), lo = tf32(x - hi); products accumulated as
 // hi*hi + hi*lo + lo*hi in fp32 in tensor memory), which keeps the error of an
 // fp32 GEMM.  k_tc_pack writes each operand tile once, already split and in the
-// swizzled shared-memory layout, so the GEMM moves whole 16 KB hi/lo tile
-// pairs with single bulk copies.
+// swizzled shared-memory layout; the GEMM moves whole 16 KB hi/lo tile pairs
+// with single bulk copies.
 
 static_assert(tc::kCols == kTcK && tc::kTileFloats == kTcTileFloats, "packed tile geometry");
 
-// One 128 x 16 tile: L21 rows (which 0) or U12 columns (which 1) of node s.
-__global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* fronts, float* pack, int64_t i0) {
+// Float offset of tile (t, kb) of a node's pack region: 0 = RA (mt x kt: F21,
+// later Pb), 1 = RB (mt x kt: F12^T), 2 = RC (nt x kt: inv(U11), later X),
+// 3 = RD (nt x kt: inv(L11)^T, later X^T).
+__device__ __forceinline__ int64_t tc_tile(int region, int t, int kb, int mt, int nt, int kt) {
+  const int64_t base = region == 0   ? 0
+                       : region == 1 ? (int64_t)mt * kt
+                       : region == 2 ? 2LL * mt * kt
+                                     : 2LL * mt * kt + (int64_t)nt * kt;
+  return (base + (int64_t)t * kt + kb) * (2 * tc::kTileFloats);
+}
+
+// One 128 x 16 operand tile.  A-side operands (rows x K, read along rows):
+// op 0 F21, op 2 inv(U11), op 4 X, op 6 Pb.  B-side operands (columns x K,
+// read down columns): op 1 F12^T, op 3 inv(L11)^T (unit diagonal), op 5 X^T.
+__global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* fronts, const float* factors,
+                                                 float* pack, int64_t i0, int inst_base) {
   const int4 it = D.items[i0 + blockIdx.x];
-  const int s = it.x, which = it.y, t = it.z, kb = it.w;
-  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
-  const int mt = (m + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
+  const int s = it.x, op = it.y, t = it.z, kb = it.w;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s];
+  const int mt = (m + 127) / 128, nt = (n + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
   const float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
-  float* dst = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s] +
-               ((int64_t)which * mt * kt + (int64_t)t * kt + kb) * (2 * tc::kTileFloats);
+  const float* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+  const int region = (op == 0 || op == 6) ? 0 : op == 1 ? 1 : (op == 2 || op == 4) ? 2 : 3;
+  const int rows = (op == 0 || op == 1 || op == 6) ? m : n;
+  const bool bside = op == 1 || op == 3 || op == 5;
+  float* dst = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s] + tc_tile(region, t, kb, mt, nt, kt);
   for (int q = threadIdx.x; q < tc::kRows * (tc::kCols / 4); q += blockDim.x) {
-    // A: 4 consecutive threads read one 64-byte row segment; B: consecutive
-    // threads read consecutive columns of one U12 row.
-    const int r = which == 0 ? q >> 2 : q & 127;
-    const int c = which == 0 ? q & 3 : q >> 7;
+    // A side: 4 consecutive threads read one 64-byte row segment; B side:
+    // consecutive threads read consecutive columns of one source row.
+    const int r = bside ? q & 127 : q >> 2;
+    const int c = bside ? q >> 7 : q & 3;
     const int row = t * tc::kRows + r;
     const int k = kb * tc::kCols + c * 4;
     float v[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
+      const int kk = k + u;
       float x = 0.f;
-      if (row < m && k + u < n)
-        x = which == 0 ? F[(int64_t)(n + row) * ldf + k + u] : F[(int64_t)(k + u) * ldf + n + row];
+      if (row < rows && kk < n) {
+        switch (op) {
+          case 0: x = F[(int64_t)(n + row) * ldf + kk]; break;
+          case 1: x = F[(int64_t)kk * ldf + n + row]; break;
+          case 2: x = kk >= row ? SQ[(int64_t)row * ldn + kk] : 0.f; break;
+          case 3: x = row < kk ? SQ[(int64_t)kk * ldn + row] : (row == kk ? 1.f : 0.f); break;
+          case 4: x = F[(int64_t)row * ldf + kk]; break;
+          case 5: x = F[(int64_t)kk * ldf + row]; break;
+          default: x = SQ[(int64_t)(n + row) * ldn + kk]; break;
+        }
+      }
       v[u] = x;
     }
     float4 hi, lo;
@@ -657,16 +654,17 @@ constexpr int kTcStageBytes = 4 * tc::kTileBytes;  // A hi, A lo, B hi, B lo
 constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 512;
 constexpr long long kTcWaitLimit = 1LL << 22;
 
-// One 128 x 128 output tile of F22 per CTA, two CTAs per SM (96 KB ring and
-// 128 TMEM columns each) so that one CTA's epilogue overlaps the other's main
-// loop.  Warp 0 lane 0 streams the k-blocks into a 3-stage ring, warp 1 lane 0
-// issues the MMAs, all four warps read the accumulator back (warp w owns TMEM
-// lanes 32w..32w+31 = tile rows) and stage it through shared memory so that
-// the read-modify-write of F22 goes row by row, coalesced.  Every wait is
-// bounded; on a timeout the CTA lets its copies land, skips the update,
-// raises ORBIT_ERR_TIMEOUT and frees its tensor memory.
-__global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts, const float* pack, int64_t i0,
-                                                     int* status) {
+// One 128 x 128 output tile per CTA of job 0 (X, written over F11), 1 (Pb,
+// into the factor storage), 2 (Qr, into the factor storage) or 3 (F22 += Pb
+// F12).  Two CTAs per SM (96 KB ring and 128 TMEM columns each) so that one
+// CTA's epilogue overlaps the other's main loop.  Warp 0 lane 0 streams the
+// k-blocks into a 3-stage ring, warp 1 lane 0 issues the MMAs, all four warps
+// read the accumulator back (warp w owns TMEM lanes 32w..32w+31 = tile rows)
+// and stage it through shared memory so that the output goes row by row,
+// coalesced.  Every wait is bounded; on a timeout the CTA lets its copies
+// land, skips the update, raises ORBIT_ERR_TIMEOUT and frees its tensor memory.
+__global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, float* factors, const float* pack,
+                                                    int64_t i0, int inst_base, int* status) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t full[kTcStages], empty[kTcStages], done;
   __shared__ uint32_t tmem_base;
@@ -674,12 +672,19 @@ __global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts,
   const uint32_t raw = tc::smem_u32(smem_raw);
   unsigned char* sbuf = smem_raw + ((512u - (raw & 511u)) & 511u);
   const int4 it = D.items[i0 + blockIdx.x];
-  const int s = it.x, tr = it.y, tcol = it.z;
-  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
-  const int kt = (n + tc::kCols - 1) / tc::kCols, mt = (m + 127) / 128;
+  const int s = it.x, tr = it.y, tcol = it.z, job = it.w;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s], ldm = D.ldm[s];
+  const int mt = (m + 127) / 128, nt = (n + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
+  const int ra = (job == 0 || job == 2) ? 2 : 0;
+  const int rb = (job == 0 || job == 1) ? 3 : 1;
+  const int M = (job == 0 || job == 2) ? n : m;
+  const int N = (job == 0 || job == 1) ? n : m;
+  // X = inv(U11) inv(L11): both factors vanish below k = max(row, column)
+  const int kb0 = job == 0 ? (tc::kRows / tc::kCols) * max(tr, tcol) : 0;
+  const int nk = kt - kb0;
   const float* pk = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s];
-  const float* pa = pk + (int64_t)tr * kt * (2 * tc::kTileFloats);
-  const float* pb = pk + ((int64_t)mt * kt + (int64_t)tcol * kt) * (2 * tc::kTileFloats);
+  const float* pa = pk + tc_tile(ra, tr, kb0, mt, nt, kt);
+  const float* pb = pk + tc_tile(rb, tcol, kb0, mt, nt, kt);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kTcStages; ++i) {
@@ -700,7 +705,7 @@ __global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts,
   const uint32_t tmem = tmem_base;
   if (threadIdx.x == 0) {
     int issued = 0;
-    for (int kb = 0; kb < kt; ++kb) {
+    for (int kb = 0; kb < nk; ++kb) {
       const int st = kb % kTcStages;
       if (kb >= kTcStages && !tc::mbar_wait(&empty[st], ((kb / kTcStages) - 1) & 1, kTcWaitLimit)) {
         failed = 1;
@@ -718,7 +723,7 @@ __global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts,
       if (!tc::mbar_wait(&full[kb % kTcStages], (kb / kTcStages) & 1, kTcWaitLimit)) failed = 1;
   } else if (threadIdx.x == 32) {
     const uint32_t idesc = tc::idesc_tf32(128, 128);
-    for (int kb = 0; kb < kt; ++kb) {
+    for (int kb = 0; kb < nk; ++kb) {
       const int st = kb % kTcStages;
       if (!tc::mbar_wait(&full[st], (kb / kTcStages) & 1, kTcWaitLimit)) {
         failed = 1;
@@ -742,13 +747,29 @@ __global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts,
   tc::fence_after_sync();
   const int good = __syncthreads_and(ok ? 1 : 0) && !failed;
   if (good) {
+    float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+    float* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
+    float* C;
+    int ldc;
+    if (job == 0) {
+      C = F;
+      ldc = ldf;
+    } else if (job == 1) {
+      C = SQ + (int64_t)n * ldn;
+      ldc = ldn;
+    } else if (job == 2) {
+      C = SQ + (int64_t)(n + m) * ldn;
+      ldc = ldm;
+    } else {
+      C = F + (int64_t)n * ldf + n;
+      ldc = ldf;
+    }
     // the ring is idle now: each warp transposes its 32 x 32 accumulator
     // blocks through a private padded buffer
     float* sw = reinterpret_cast<float*>(sbuf) + warp * 32 * 33;
-    const int rows = min(32, m - tr * tc::kRows - warp * 32);
-    const int cols = min(128, m - tcol * 128);
-    float* C = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s] +
-               (int64_t)(n + tr * tc::kRows + warp * 32) * ldf + n + tcol * 128;
+    const int rows = min(32, M - tr * tc::kRows - warp * 32);
+    const int cols = min(128, N - tcol * 128);
+    C += (int64_t)(tr * tc::kRows + warp * 32) * ldc + tcol * 128;
     for (int cc = 0; cc < 4 && cc * 32 < cols; ++cc) {
       float v[32];
       tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
@@ -757,14 +778,19 @@ __global__ void __launch_bounds__(128, 2) k_schur_tc(FactorDev D, float* fronts,
       __syncwarp();
       const int col = cc * 32 + lane;
       if (col < cols) {
-        for (int r0 = 0; r0 < rows; r0 += 8) {
-          float c[8];
+        if (job == 3) {
+          for (int r0 = 0; r0 < rows; r0 += 8) {
+            float c[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
-            if (r0 + u < rows) c[u] = C[(int64_t)(r0 + u) * ldf + col];
+            for (int u = 0; u < 8; ++u)
+              if (r0 + u < rows) c[u] = C[(int64_t)(r0 + u) * ldc + col];
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
-            if (r0 + u < rows) C[(int64_t)(r0 + u) * ldf + col] = c[u] - sw[(r0 + u) * 33 + lane];
+            for (int u = 0; u < 8; ++u)
+              if (r0 + u < rows) C[(int64_t)(r0 + u) * ldc + col] = c[u] + sw[(r0 + u) * 33 + lane];
+          }
+        } else {
+          const float sg = job == 0 ? 1.f : -1.f;
+          for (int r = 0; r < rows; ++r) C[(int64_t)r * ldc + col] = sg * sw[r * 33 + lane];
         }
       }
       __syncwarp();
@@ -798,6 +824,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   D.group = f->front_group;
   D.tc_pack_off = sy->d.tc_pack_off;
   D.tc_pack_stride = S.tc_pack_size;
+  D.tc_min_n = INT_MAX;
   T* factors = reinterpret_cast<T*>(f->factors);
   T* fronts = reinterpret_cast<T*>(f->fronts);
   const int n_inst = n_active * f->n_bins;
@@ -810,7 +837,11 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   if constexpr (std::is_same<T, float>::value) {
     const char* e = std::getenv("ORBIT_B200_TC");
     use_tc = f->tc_pack != nullptr && !(e && e[0] == '0');
-    if (use_tc) { int _r = allow_max_smem((const void*)k_schur_tc); if (_r) return _r; }
+    if (use_tc) {
+      int _r = allow_max_smem((const void*)k_gemm_tc);
+      if (_r) return _r;
+      D.tc_min_n = S.tc_min_n;
+    }
   }
   { int _r = allow_max_smem((const void*)k_prod2<T>); if (_r) return _r; }
   { int _r = allow_max_smem((const void*)k_update2<T>); if (_r) return _r; }
@@ -864,7 +895,17 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
           if constexpr (std::is_same<T, float>::value) {
             if (use_tc) {
               dim3 g((unsigned)L.items, G);
-              k_tc_pack<<<g, 256, 0, st>>>(D, cur, f->tc_pack, L.item_off);
+              k_tc_pack<<<g, 256, 0, st>>>(D, cur, factors, f->tc_pack, L.item_off, base);
+              note_launch();
+            }
+          }
+          break;
+        }
+        case FactorLaunch::TC_GEMM: {
+          if constexpr (std::is_same<T, float>::value) {
+            if (use_tc) {
+              dim3 g((unsigned)L.items, G);
+              k_gemm_tc<<<g, 128, kTcSmem, st>>>(D, cur, factors, f->tc_pack, L.item_off, base, f->status);
               note_launch();
             }
           }
@@ -876,13 +917,6 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
             dim3 g((unsigned)n_cc, G);
             k_schur<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off);
             note_launch();
-          }
-          if constexpr (std::is_same<T, float>::value) {
-            if (use_tc && L.items > L.p0) {
-              dim3 g((unsigned)(L.items - L.p0), G);
-              k_schur_tc<<<g, 128, kTcSmem, st>>>(D, cur, f->tc_pack, L.item_off + L.p0, f->status);
-              note_launch();
-            }
           }
           break;
         }

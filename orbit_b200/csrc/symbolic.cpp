@@ -18,6 +18,7 @@
 #include <array>
 #include <cmath>
 #include <functional>
+#include <initializer_list>
 
 namespace orbit {
 
@@ -283,6 +284,11 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
   auto nitems = [&]() { return int64_t(S.fitems.size() / 4); };
   for (int l = S.nlevels - 1; l >= 0; --l) {
     const auto& sups = S.level_sups[l];
+    std::vector<int> small, big;  // tensor-core nodes: n >= tc_min_n and m > 0
+    for (int s : sups) {
+      if (S.m[s] == 0 || S.n[s] == 0) continue;
+      (S.n[s] >= S.tc_min_n ? big : small).push_back(s);
+    }
     {
       // every front row written once: the children's Schur complements
       // gathered through the inverse maps, zeros elsewhere; then the stencil
@@ -331,27 +337,10 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
       if (nitems() > off) S.fsched.push_back({FactorLaunch::UPDATE, l, p0, off, nitems() - off});
     }
     {
-      // Schur complements: nodes below the tensor-core threshold first (their
-      // item count goes in p0), then the tensor-core nodes, whose operands a
-      // TC_PACK launch packs first.
-      std::vector<int> small, big;
-      for (int s : sups) {
-        if (S.m[s] == 0 || S.n[s] == 0) continue;
-        (S.n[s] >= S.tc_min_n ? big : small).push_back(s);
-      }
-      int64_t pack = 0;
+      // Schur complements on the CUDA cores: nodes below the tensor-core
+      // threshold first (their item count goes in p0), then the tensor-core
+      // nodes, which an fp32 factorization handles in its own pipeline below.
       int64_t off = nitems();
-      for (int s : big) {
-        const int mt = (S.m[s] + kSchurTile - 1) / kSchurTile, kt = (S.n[s] + kTcK - 1) / kTcK;
-        S.tc_pack_off[s] = pack;
-        pack += int64_t(2) * mt * kt * 2 * kTcTileFloats;
-        for (int which = 0; which < 2; ++which)
-          for (int t = 0; t < mt; ++t)
-            for (int k = 0; k < kt; ++k) push_item(s, which, t, k);
-      }
-      S.tc_pack_size = std::max(S.tc_pack_size, pack);
-      if (nitems() > off) S.fsched.push_back({FactorLaunch::TC_PACK, l, 0, off, nitems() - off});
-      off = nitems();
       int nsmall = 0;
       for (int pass = 0; pass < 2; ++pass)
         for (int s : pass == 0 ? small : big) {
@@ -398,6 +387,55 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
       }
       if (nitems() > off)
         S.fsched.push_back({which == 0 ? FactorLaunch::PRODL : FactorLaunch::PRODU, l, 0, off, nitems() - off});
+    }
+    // Tensor-core pipeline of the fp32 factorization for the big nodes, whose
+    // LU the panel/update launches above confined to F11 (F21, F12 stay as
+    // assembled): X = inv(U11) inv(L11); Pb = -F21 X; Qr = -X F12; then the
+    // Schur complement F22 += Pb F12.  Each GEMM reads operands packed as tf32
+    // hi/lo tiles; pack items are {s, op, tile, k-block}, GEMM items
+    // {s, row tile, column tile, job}.  Per node the pack holds regions
+    // RA (mt x kt tiles: F21, later Pb), RB (mt x kt: F12^T) and RC
+    // (2 x nt x kt: inv(U11) and inv(L11)^T, later X and X^T).
+    if (!big.empty()) {
+      int64_t pack = 0;
+      for (int s : big) {
+        const int64_t mt = (S.m[s] + kSchurTile - 1) / kSchurTile, nt = (S.n[s] + kSchurTile - 1) / kSchurTile;
+        const int64_t kt = (S.n[s] + kTcK - 1) / kTcK;
+        S.tc_pack_off[s] = pack;
+        pack += (2 * mt + 2 * nt) * kt * 2 * kTcTileFloats;
+      }
+      S.tc_pack_size = std::max(S.tc_pack_size, pack);
+      auto pack_launch = [&](std::initializer_list<int> ops) {
+        const int64_t off = nitems();
+        for (int s : big) {
+          const int mt = (S.m[s] + kSchurTile - 1) / kSchurTile, nt = (S.n[s] + kSchurTile - 1) / kSchurTile;
+          const int kt = (S.n[s] + kTcK - 1) / kTcK;
+          for (int op : ops) {
+            const int tiles = (op == 0 || op == 1 || op == 6) ? mt : nt;
+            for (int t = 0; t < tiles; ++t)
+              for (int k = 0; k < kt; ++k) push_item(s, op, t, k);
+          }
+        }
+        S.fsched.push_back({FactorLaunch::TC_PACK, l, 0, off, nitems() - off});
+      };
+      auto gemm_launch = [&](std::initializer_list<int> jobs) {
+        const int64_t off = nitems();
+        for (int s : big) {
+          const int mt = (S.m[s] + kSchurTile - 1) / kSchurTile, nt = (S.n[s] + kSchurTile - 1) / kSchurTile;
+          for (int job : jobs) {
+            const int rows = (job == 0 || job == 2) ? nt : mt, cols = (job == 0 || job == 1) ? nt : mt;
+            for (int a = 0; a < rows; ++a)
+              for (int b = 0; b < cols; ++b) push_item(s, a, b, job);
+          }
+        }
+        S.fsched.push_back({FactorLaunch::TC_GEMM, l, 0, off, nitems() - off});
+      };
+      pack_launch({0, 1, 2, 3});  // F21, F12^T, inv(U11), inv(L11)^T
+      gemm_launch({0});           // X
+      pack_launch({4, 5});        // X, X^T
+      gemm_launch({1, 2});        // Pb, Qr
+      pack_launch({6});           // Pb
+      gemm_launch({3});           // Schur complement
     }
   }
 

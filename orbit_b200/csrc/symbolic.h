@@ -31,7 +31,7 @@ inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 // One kernel launch of the numeric factorization schedule.
 struct FactorLaunch {
-  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU, TC_PACK, ASSEMBLE } kind;
+  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU, TC_PACK, ASSEMBLE, TC_GEMM } kind;
   int level;
   int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV); SCHUR: leading items of CUDA-core nodes
   int64_t item_off;  // offset into the item array (int4 units)
@@ -90,10 +90,9 @@ struct Symbolic {
   int max_sub_front = 0;  // largest n+m of a supernode inside a subtree task
   int max_nm = 0;
   double factor_flops = 0.0;
-  // tensor-core Schur complements (fp32 factors): supernodes with n >= tc_min_n
-  // have their L21 and U12^T packed as tf32 hi/lo tile pairs; tc_pack_off[s] is
-  // the float offset of that pack inside its level's per-instance pack buffer
-  // (A tiles [mt][kt][hi|lo], then B tiles [nt][kt][hi|lo]), -1 for others.
+  // tensor-core pipeline (fp32 factors) for supernodes with n >= tc_min_n and
+  // m > 0: tc_pack_off[s] is the float offset of the node's tf32 hi/lo operand
+  // tiles inside its level's per-instance pack buffer, -1 for other nodes.
   int tc_min_n = 0;
   std::vector<int64_t> tc_pack_off;
   int64_t tc_pack_size = 0;  // floats per instance (max over levels)
