@@ -161,16 +161,22 @@ __global__ void k_copy_A(double* A, const double* const* Tp, const double* const
 // children's Schur-complement rows mapped through the inverse extend-add maps
 // (zero where no child contributes), written once together with its padding
 // columns.  The stencil entries are added afterwards (k_scatter).  One warp
-// per row: the stores are contiguous and the children's rows are read in
-// increasing column order.
+// per row, four consecutive columns per lane: the maps are read from shared
+// memory as int4, the row is stored with 16-byte stores (rows start 16-byte
+// aligned), and the children's rows are read in increasing column order.
 template <typename T>
 __global__ void __launch_bounds__(256) k_assemble(FactorDev D, T* fr, const T* fr_child, int64_t i0) {
-  extern __shared__ int32_t sinv[];  // 2 x (n + m)
+  extern __shared__ int4 sinv4[];  // map of child 0 at [0, wp), child 1 at [wp, 2 wp)
+  int32_t* sinv = reinterpret_cast<int32_t*>(sinv4);
   const int4 it = D.items[i0 + blockIdx.x];
   const int s = it.x, r0 = it.y, r1 = it.z;
   const int n = D.n[s], m = D.m[s], w = n + m, ldf = D.ldf[s];
+  const int wp = (w + 3) & ~3;  // <= ldf
   const int32_t* gi = D.ginv + D.ginv_off[s];
-  for (int j = threadIdx.x; j < 2 * w; j += blockDim.x) sinv[j] = gi[j];
+  for (int j = threadIdx.x; j < 2 * wp; j += blockDim.x) {
+    const int q = j >= wp, jj = j - q * wp;
+    sinv[j] = jj < w ? gi[q * w + jj] : -1;
+  }
   __syncthreads();
   T* F = fr + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   const T* Sc[2] = {nullptr, nullptr};
@@ -183,25 +189,42 @@ __global__ void __launch_bounds__(256) k_assemble(FactorDev D, T* fr, const T* f
       Sc[q] = fr_child + (int64_t)blockIdx.y * D.front_buf + D.front_off[c] + (int64_t)D.n[c] * ldc[q] + D.n[c];
     }
   }
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int VW = 16 / sizeof(T);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = r0 + warp; i < r1; i += blockDim.x / 32) {
-    const int u0 = sinv[i], u1 = sinv[w + i];
+    const int u0 = sinv[i], u1 = sinv[wp + i];
     const T* s0 = u0 >= 0 ? Sc[0] + (int64_t)u0 * ldc[0] : nullptr;
     const T* s1 = u1 >= 0 ? Sc[1] + (int64_t)u1 * ldc[1] : nullptr;
     T* row = F + (int64_t)i * ldf;
-    for (int j = lane; j < ldf; j += 32) {
-      T v = T(0);
-      if (j < w) {
+    for (int j0 = 4 * lane; j0 < ldf; j0 += 128) {
+      T v[4] = {T(0), T(0), T(0), T(0)};
+      if (j0 < wp) {
         if (s0) {
-          const int v0 = sinv[j];
-          if (v0 >= 0) v += s0[v0];
+          const int4 c = sinv4[j0 >> 2];
+          if (c.x >= 0) v[0] += s0[c.x];
+          if (c.y >= 0) v[1] += s0[c.y];
+          if (c.z >= 0) v[2] += s0[c.z];
+          if (c.w >= 0) v[3] += s0[c.w];
         }
         if (s1) {
-          const int v1 = sinv[w + j];
-          if (v1 >= 0) v += s1[v1];
+          const int4 c = sinv4[(wp + j0) >> 2];
+          if (c.x >= 0) v[0] += s1[c.x];
+          if (c.y >= 0) v[1] += s1[c.y];
+          if (c.z >= 0) v[2] += s1[c.z];
+          if (c.w >= 0) v[3] += s1[c.w];
         }
       }
-      row[j] = v;
+#pragma unroll
+      for (int h = 0; h < 4; h += VW) {
+        V x;
+        if constexpr (VW == 4) {
+          x.x = v[0]; x.y = v[1]; x.z = v[2]; x.w = v[3];
+        } else {
+          x.x = v[h]; x.y = v[h + 1];
+        }
+        *reinterpret_cast<V*>(row + j0 + h) = x;
+      }
     }
   }
 }
@@ -862,7 +885,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
       switch (L.kind) {
         case FactorLaunch::ASSEMBLE: {
           dim3 g((unsigned)L.items, G);
-          k_assemble<T><<<g, 256, sizeof(int32_t) * 2 * S.max_front, st>>>(D, cur, chl, L.item_off);
+          k_assemble<T><<<g, 256, sizeof(int32_t) * 2 * (S.max_front + 4), st>>>(D, cur, chl, L.item_off);
           note_launch();
           break;
         }

@@ -274,7 +274,7 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     }
 
   // ---- factorization schedule ----
-  S.tc_min_n = 96;
+  S.tc_min_n = 48;
   if (const char* e = std::getenv("ORBIT_B200_TC_MIN_N")) S.tc_min_n = std::max(1, std::atoi(e));
   S.tc_pack_off.assign(ns, -1);
   S.tc_pack_size = 0;
