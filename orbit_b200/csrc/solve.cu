@@ -36,11 +36,14 @@ namespace {
 #define ORBIT_SOLVE_MINB 8
 #endif
 constexpr int kSolveThreads = ORBIT_SOLVE_THREADS;
+constexpr int kMaxPhases = 96;  // 2 x tree levels
 constexpr int kWarps = kSolveThreads / 32;
 
 template <typename T>
 struct ChainDev {
   const int32_t *first, *n, *m, *parent, *child, *uidx, *rel, *ldn, *ldm;
+  const int32_t* ginv;      // inverse extend-add maps, 2 x (n + m) per supernode
+  const int64_t* ginv_off;
   const int32_t *nch_f, *nch_b, *level;
   int sub_front;  // per-warp vector capacity for subtree tasks
   const int64_t *uoff, *fac_off, *woff;
@@ -184,22 +187,31 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
     if (!trans) Ein = D.E + ((int64_t)o * 8 + tau) * N;
     else if (tau + 1 < D.tau1) Ein = D.E + ((int64_t)o * 8 + tau + 1) * N;
   }
-  for (int i = tid; i < n + m; i += kSolveThreads) {
-    double v = 0.0;
-    if (i < n) {
-      v = Xin[first + i];
-      if (Ein) v += D.escale * Ein[first + i];
-    }
+  // Rows (or columns) [r0, r1) read vec on [0, min(r1, n)) and on
+  // [max(r0, n), r1): only that part is gathered, in one pass, each position
+  // pulling its own entry and the children's update entries that land on it
+  // (inverse extend-add maps, -1 where a child contributes nothing).
+  const int lo_end = min(r1, n), hi0 = max(r0, n);
+  const int w = n + m;
+  const int32_t* g0 = D.ginv + D.ginv_off[s];
+  const int32_t* g1 = g0 + w;
+  const int c0 = D.child[2 * s], c1 = D.child[2 * s + 1];
+  const double* W0 = c0 >= 0 ? Wo + D.woff[c0] : nullptr;
+  const double* W1 = c1 >= 0 ? Wo + D.woff[c1] : nullptr;
+  for (int i = tid; i < lo_end; i += kSolveThreads) {
+    double v = Xin[first + i];
+    if (Ein) v += D.escale * Ein[first + i];
+    const int u0 = g0[i], u1 = g1[i];
+    if (u0 >= 0) v += W0[u0];
+    if (u1 >= 0) v += W1[u1];
     vec[i] = (T)v;
   }
-  for (int q2 = 0; q2 < 2; ++q2) {
-    __syncthreads();
-    const int c = D.child[2 * s + q2];
-    if (c < 0) continue;
-    const int mc = D.m[c];
-    const int32_t* rel = D.rel + D.uoff[c];
-    const double* wc = Wo + D.woff[c];
-    for (int j = tid; j < mc; j += kSolveThreads) vec[rel[j]] += (T)wc[j];
+  for (int i = hi0 + tid; i < r1; i += kSolveThreads) {
+    double v = 0.0;
+    const int u0 = g0[i], u1 = g1[i];
+    if (u0 >= 0) v += W0[u0];
+    if (u1 >= 0) v += W1[u1];
+    vec[i] = (T)v;
   }
   __syncthreads();
   if (!trans) {
@@ -260,7 +272,8 @@ __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
   const int bin_out = trans ? tau : tau + 1;
   double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
   const int32_t* ui = D.uidx + D.uoff[s];
-  for (int i = tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
+  // rows (or columns) [r0, r1) read the own part of vec from r0 on
+  for (int i = r0 + tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
   for (int u = tid; u < m; u += kSolveThreads) vec[n0pad + u] = (T)Xout[ui[u]];
   __syncthreads();
   if (!trans) {
@@ -416,8 +429,10 @@ __global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(Chain
   T* vec = red + kWarps * 32;                    // front-sized vector
   __shared__ int s_task;
   __shared__ int s_ok;
+  __shared__ int s_phase[kMaxPhases + 1];  // phase offsets x B
   const int tid = threadIdx.x;
   const int per_bin = D.items_per_bin * D.B;
+  for (int i = tid; i <= D.nphase; i += blockDim.x) s_phase[i] = D.phase_off[i] * D.B;
   for (;;) {
     if (tid == 0) {
       s_task = atomicAdd(D.task_counter, 1);
@@ -429,9 +444,14 @@ __global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(Chain
     const int q = t / per_bin;
     const int r = t - q * per_bin;
     const int tau = D.trans ? (D.tau1 - 1 - q) : (D.tau0 + q);
-    int p = 0;
-    while (D.phase_off[p + 1] * D.B <= r) ++p;
-    const int rr = r - D.phase_off[p] * D.B;
+    int lo = 0, hi = D.nphase;  // phase p with s_phase[p] <= r < s_phase[p + 1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_phase[mid] <= r) lo = mid;
+      else hi = mid;
+    }
+    const int p = lo;
+    const int rr = r - s_phase[p];
     const int cnt = D.phase_off[p + 1] - D.phase_off[p];
     const int oi = rr / cnt;
     const int4 it = D.items[D.phase_off[p] + (rr - oi * cnt)];
@@ -519,6 +539,7 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   ChainDev<T> D;
   D.first = sy->d.first; D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent;
   D.child = sy->d.child; D.uidx = sy->d.uidx; D.rel = sy->d.rel; D.ldn = sy->d.ldn; D.ldm = sy->d.ldm;
+  D.ginv = sy->d.ginv; D.ginv_off = sy->d.ginv_off;
   D.nch_f = trans ? sy->d.nchunk_fwdT : sy->d.nchunk_fwd;
   D.nch_b = trans ? sy->d.nchunk_bwdT : sy->d.nchunk_bwd;
   D.level = sy->d.level;
@@ -527,6 +548,10 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.items = trans ? sy->d.sitems + S.items_per_bin : sy->d.sitems;
   D.phase_off = trans ? sy->d.phase_offT : sy->d.phase_off;
   D.nphase = 2 * S.nlevels;
+  if (D.nphase > kMaxPhases) {
+    set_last_error("chained solve: supernode tree deeper than the kernel's phase table");
+    return ORBIT_ERR_INTERNAL;
+  }
   D.items_per_bin = trans ? S.items_per_binT : S.items_per_bin;
   D.nsuper = S.nsuper;
   D.N = S.N; D.fac_size = S.fac_size; D.w_size = S.w_size;

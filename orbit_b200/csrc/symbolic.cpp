@@ -182,6 +182,11 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
       S.rel[S.uoff[s] + q] = pos;
     }
   }
+  // the solve's gathers rely on increasing extend-add maps (a parent's own
+  // unknowns precede its ancestors in the elimination order)
+  for (int s = 0; s < ns; ++s)
+    for (int64_t q = S.uoff[s] + 1; q < S.uoff[s + 1]; ++q)
+      if (S.rel[q] <= S.rel[q - 1]) return "internal: extend-add map not increasing";
   S.ginv_off.assign(ns + 1, 0);
   for (int s = 0; s < ns; ++s) S.ginv_off[s + 1] = S.ginv_off[s] + 2 * int64_t(S.n[s] + S.m[s]);
   S.ginv.assign(S.ginv_off[ns], -1);

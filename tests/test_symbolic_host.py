@@ -135,8 +135,11 @@ def test_structure(shape, leaf):
         assert np.all(np.diff(u) > 0)
         assert np.all(u >= first[s] + n[s])  # only later (ancestor) unknowns
     assert sym.lunz == int((n.astype(np.int64) ** 2 + 2 * n.astype(np.int64) * m).sum())
-    # inverse extend-add maps: ginv[s][q][rel_c[u]] == u for child q, -1 elsewhere
     child, rel, ginv, goff = sym.array("child"), sym.array("rel"), sym.array("ginv"), sym.array("ginv_off")
+    # extend-add maps increase (the solve's gathers stop at the first entry past a chunk)
+    for s in range(len(n)):
+        assert np.all(np.diff(rel[uoff[s]:uoff[s + 1]]) > 0)
+    # inverse extend-add maps: ginv[s][q][rel_c[u]] == u for child q, -1 elsewhere
     for s in range(len(n)):
         w = int(n[s] + m[s])
         inv = ginv[goff[s]:goff[s] + 2 * w].reshape(2, w)
