@@ -118,16 +118,20 @@ int build_device_symbolic(orbit_symbolic_s* h) {
     std::vector<int4> fi(S.fitems.size() / 4);
     std::memcpy(fi.data(), S.fitems.data(), fi.size() * sizeof(int4));
     ORBIT_TRY(upload(A, &d.fitems, fi));
-    std::vector<int4> si(S.sitems.size() / 4);
-    std::memcpy(si.data(), S.sitems.data(), si.size() * sizeof(int4));
-    ORBIT_TRY(upload(A, &d.sitems, si));
   }
-  ORBIT_TRY(upload(A, &d.phase_off, S.phase_off));
-  ORBIT_TRY(upload(A, &d.phase_offT, S.phase_offT));
-  ORBIT_TRY(upload(A, &d.nchunk_fwd, S.nchunk_fwd));
-  ORBIT_TRY(upload(A, &d.nchunk_bwd, S.nchunk_bwd));
-  ORBIT_TRY(upload(A, &d.nchunk_fwdT, S.nchunk_fwdT));
-  ORBIT_TRY(upload(A, &d.nchunk_bwdT, S.nchunk_bwdT));
+  for (int k = 0; k < kNumSched; ++k) {
+    const SolveSched& Q = S.sched[k];
+    auto& q = d.sched[k];
+    std::vector<int4> si(Q.sitems.size() / 4);
+    std::memcpy(si.data(), Q.sitems.data(), si.size() * sizeof(int4));
+    ORBIT_TRY(upload(A, &q.sitems, si));
+    ORBIT_TRY(upload(A, &q.phase_off, Q.phase_off));
+    ORBIT_TRY(upload(A, &q.phase_offT, Q.phase_offT));
+    ORBIT_TRY(upload(A, &q.nchunk_fwd, Q.nchunk_fwd));
+    ORBIT_TRY(upload(A, &q.nchunk_bwd, Q.nchunk_bwd));
+    ORBIT_TRY(upload(A, &q.nchunk_fwdT, Q.nchunk_fwdT));
+    ORBIT_TRY(upload(A, &q.nchunk_bwdT, Q.nchunk_bwdT));
+  }
   ORBIT_TRY(upload(A, &d.perm, S.perm));
   ORBIT_TRY(upload(A, &d.iperm, S.iperm));
   ORBIT_TRY(upload(A, &d.level, S.level));
@@ -238,7 +242,7 @@ int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info) {
   }
   const Symbolic& S = sym->S;
   int64_t v[13] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
-                   (int64_t)S.factor_flops, S.items_per_bin, S.w_size, S.leaf_cells, S.max_nm,
+                   (int64_t)S.factor_flops, S.sched[1].items_per_bin, S.w_size, S.leaf_cells, S.max_nm,
                    S.max_sub_front};
   for (int i = 0; i < n_info && i < 13; ++i) info[i] = v[i];
   return ORBIT_OK;
@@ -268,10 +272,10 @@ int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int6
   ORBIT_ARR("front_off", front_off) ORBIT_ARR("level_front_size", level_front_size)
   ORBIT_ARR("ent_level_off", ent_level_off) ORBIT_ARR("ent_pos", ent_pos) ORBIT_ARR("ent_src", ent_src)
   ORBIT_ARR("ginv", ginv) ORBIT_ARR("ginv_off", ginv_off)
-  ORBIT_ARR("woff", woff) ORBIT_ARR("sitems", sitems) ORBIT_ARR("phase_off", phase_off)
-  ORBIT_ARR("phase_offT", phase_offT) ORBIT_ARR("nchunk_fwd", nchunk_fwd)
-  ORBIT_ARR("nchunk_bwd", nchunk_bwd) ORBIT_ARR("nchunk_fwdT", nchunk_fwdT)
-  ORBIT_ARR("nchunk_bwdT", nchunk_bwdT)
+  ORBIT_ARR("woff", woff) ORBIT_ARR("sitems", sched[1].sitems) ORBIT_ARR("phase_off", sched[1].phase_off)
+  ORBIT_ARR("phase_offT", sched[1].phase_offT) ORBIT_ARR("nchunk_fwd", sched[1].nchunk_fwd)
+  ORBIT_ARR("nchunk_bwd", sched[1].nchunk_bwd) ORBIT_ARR("nchunk_fwdT", sched[1].nchunk_fwdT)
+  ORBIT_ARR("nchunk_bwdT", sched[1].nchunk_bwdT)
 #undef ORBIT_ARR
   if (!src && cnt == 0 && nm != "sitems") {
     bool known = false;

@@ -19,9 +19,11 @@ struct DevSym {
   int64_t *ent_pos = nullptr;
   int32_t *ent_src = nullptr;
   int4 *fitems = nullptr;
-  int4 *sitems = nullptr;
-  int32_t *phase_off = nullptr, *phase_offT = nullptr;
-  int32_t *nchunk_fwd = nullptr, *nchunk_bwd = nullptr, *nchunk_fwdT = nullptr, *nchunk_bwdT = nullptr;
+  struct Sched {
+    int4 *sitems = nullptr;
+    int32_t *phase_off = nullptr, *phase_offT = nullptr;
+    int32_t *nchunk_fwd = nullptr, *nchunk_bwd = nullptr, *nchunk_fwdT = nullptr, *nchunk_bwdT = nullptr;
+  } sched[orbit::kNumSched];
   int32_t *perm = nullptr, *iperm = nullptr;
   int32_t *level = nullptr;
   int64_t *tc_pack_off = nullptr;

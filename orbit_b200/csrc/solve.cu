@@ -540,19 +540,24 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.first = sy->d.first; D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent;
   D.child = sy->d.child; D.uidx = sy->d.uidx; D.rel = sy->d.rel; D.ldn = sy->d.ldn; D.ldm = sy->d.ldm;
   D.ginv = sy->d.ginv; D.ginv_off = sy->d.ginv_off;
-  D.nch_f = trans ? sy->d.nchunk_fwdT : sy->d.nchunk_fwd;
-  D.nch_b = trans ? sy->d.nchunk_bwdT : sy->d.nchunk_bwd;
+  // schedule by batch size: small chunks shorten one orbit's critical path,
+  // large ones cut per-task overhead when many orbits fill the GPU
+  const int ks = B <= 2 ? 0 : B <= 6 ? 1 : 2;
+  const SolveSched& Q = S.sched[ks];
+  const auto& q = sy->d.sched[ks];
+  D.nch_f = trans ? q.nchunk_fwdT : q.nchunk_fwd;
+  D.nch_b = trans ? q.nchunk_bwdT : q.nchunk_bwd;
   D.level = sy->d.level;
   D.sub_front = S.max_sub_front;
   D.uoff = sy->d.uoff; D.fac_off = sy->d.fac_off; D.woff = sy->d.woff;
-  D.items = trans ? sy->d.sitems + S.items_per_bin : sy->d.sitems;
-  D.phase_off = trans ? sy->d.phase_offT : sy->d.phase_off;
+  D.items = trans ? q.sitems + Q.items_per_bin : q.sitems;
+  D.phase_off = trans ? q.phase_offT : q.phase_off;
   D.nphase = 2 * S.nlevels;
   if (D.nphase > kMaxPhases) {
     set_last_error("chained solve: supernode tree deeper than the kernel's phase table");
     return ORBIT_ERR_INTERNAL;
   }
-  D.items_per_bin = trans ? S.items_per_binT : S.items_per_bin;
+  D.items_per_bin = trans ? Q.items_per_binT : Q.items_per_bin;
   D.nsuper = S.nsuper;
   D.N = S.N; D.fac_size = S.fac_size; D.w_size = S.w_size;
   D.factors = reinterpret_cast<const T*>(f->factors);

@@ -444,28 +444,12 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     }
   }
 
-  // ---- solve schedule ----
+  // ---- solve schedules ----
   // Rows of a supernode are split into chunks of roughly `chunk_elems`
-  // matrix elements so that large separators spread over many CTAs.
-  S.nchunk_fwd.assign(ns, 0); S.nchunk_bwd.assign(ns, 0);
-  S.nchunk_fwdT.assign(ns, 0); S.nchunk_bwdT.assign(ns, 0);
-  auto chunk_rows = [&](int s, int kind, int rows, std::function<int64_t(int)> rowlen) {
-    int start = 0;
-    int cnt = 0;
-    int64_t acc = 0;
-    for (int r = 0; r < rows; ++r) {
-      acc += std::max<int64_t>(rowlen(r), 1) + 8;
-      bool last = (r == rows - 1);
-      if (acc >= chunk_elems || last || (r + 1 - start) >= 1024) {
-        S.sitems.push_back(s); S.sitems.push_back(start); S.sitems.push_back(r + 1);
-        S.sitems.push_back(kind);
-        start = r + 1;
-        acc = 0;
-        ++cnt;
-      }
-    }
-    return cnt;
-  };
+  // matrix elements so that large separators spread over many CTAs.  Three
+  // schedules (chunk/2, chunk, 2 chunk) serve small, medium and large
+  // batches: fewer, larger chunks cost less per task when many orbits keep
+  // the GPU busy, smaller ones shorten the critical path of a single orbit.
   // Subtree tasks: below a work threshold a whole subtree is one task (its
   // nodes are a contiguous postorder range), which removes the per-level
   // dependency waits of the many small supernodes near the leaves.
@@ -502,70 +486,93 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
   S.max_sub_front = 0;
   for (int s2 = 0; s2 < ns; ++s2)
     if (S.role[s2] != 0) S.max_sub_front = std::max(S.max_sub_front, S.n[s2] + S.m[s2]);
-  auto push4 = [&](int a, int b, int c, int d) {
-    S.sitems.push_back(a); S.sitems.push_back(b); S.sitems.push_back(c); S.sitems.push_back(d);
-  };
-  // non-transposed: fwd levels deep->0, bwd levels 0->deep
-  S.phase_off.clear();
-  for (int l = S.nlevels - 1; l >= 0; --l) {
-    S.phase_off.push_back(int32_t(S.sitems.size() / 4));
-    for (int s : S.level_sups[l]) {
-      int n = S.n[s], m = S.m[s];
-      if (S.role[s] == 2) continue;
-      if (S.role[s] == 1) {
-        push4(s, sub_node_first[s], 0, 4);
-        S.nchunk_fwd[s] = 1;
-        continue;
+  for (int k = 0; k < kNumSched; ++k) {
+    SolveSched& Q = S.sched[k];
+    Q.chunk_elems = k == 0 ? std::max(256, chunk_elems / 2) : k == 1 ? chunk_elems : 2 * chunk_elems;
+    Q.nchunk_fwd.assign(ns, 0); Q.nchunk_bwd.assign(ns, 0);
+    Q.nchunk_fwdT.assign(ns, 0); Q.nchunk_bwdT.assign(ns, 0);
+    auto chunk_rows = [&](int s, int kind, int rows, std::function<int64_t(int)> rowlen) {
+      int start = 0;
+      int cnt = 0;
+      int64_t acc = 0;
+      for (int r = 0; r < rows; ++r) {
+        acc += std::max<int64_t>(rowlen(r), 1) + 8;
+        bool last = (r == rows - 1);
+        if (acc >= Q.chunk_elems || last || (r + 1 - start) >= 1024) {
+          Q.sitems.push_back(s); Q.sitems.push_back(start); Q.sitems.push_back(r + 1);
+          Q.sitems.push_back(kind);
+          start = r + 1;
+          acc = 0;
+          ++cnt;
+        }
       }
-      S.nchunk_fwd[s] = chunk_rows(s, 0, n + m, [n](int r) { return r < n ? int64_t(r) : int64_t(n); });
-    }
-  }
-  for (int l = 0; l < S.nlevels; ++l) {
-    S.phase_off.push_back(int32_t(S.sitems.size() / 4));
-    for (int s : S.level_sups[l]) {
-      int n = S.n[s], m = S.m[s];
-      if (S.role[s] == 2) continue;
-      if (S.role[s] == 1) {
-        push4(s, sub_node_first[s], 0, 5);
-        S.nchunk_bwd[s] = 1;
-        continue;
+      return cnt;
+    };
+    auto push4 = [&](int a, int b, int c, int d) {
+      Q.sitems.push_back(a); Q.sitems.push_back(b); Q.sitems.push_back(c); Q.sitems.push_back(d);
+    };
+    // non-transposed: fwd levels deep->0, bwd levels 0->deep
+    Q.phase_off.clear();
+    for (int l = S.nlevels - 1; l >= 0; --l) {
+      Q.phase_off.push_back(int32_t(Q.sitems.size() / 4));
+      for (int s : S.level_sups[l]) {
+        int n = S.n[s], m = S.m[s];
+        if (S.role[s] == 2) continue;
+        if (S.role[s] == 1) {
+          push4(s, sub_node_first[s], 0, 4);
+          Q.nchunk_fwd[s] = 1;
+          continue;
+        }
+        Q.nchunk_fwd[s] = chunk_rows(s, 0, n + m, [n](int r) { return r < n ? int64_t(r) : int64_t(n); });
       }
-      S.nchunk_bwd[s] = chunk_rows(s, 1, n, [n, m](int r) { return int64_t(n - r + m); });
     }
-  }
-  S.phase_off.push_back(int32_t(S.sitems.size() / 4));
-  S.items_per_bin = S.phase_off.back();
-  // transposed: fwdT levels deep->0 over output columns (n+m), bwdT levels 0->deep over n columns
-  int32_t base = S.items_per_bin;
-  S.phase_offT.clear();
-  for (int l = S.nlevels - 1; l >= 0; --l) {
-    S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
-    for (int s : S.level_sups[l]) {
-      int n = S.n[s], m = S.m[s];
-      if (S.role[s] == 2) continue;
-      if (S.role[s] == 1) {
-        push4(s, sub_node_first[s], 0, 6);
-        S.nchunk_fwdT[s] = 1;
-        continue;
+    for (int l = 0; l < S.nlevels; ++l) {
+      Q.phase_off.push_back(int32_t(Q.sitems.size() / 4));
+      for (int s : S.level_sups[l]) {
+        int n = S.n[s], m = S.m[s];
+        if (S.role[s] == 2) continue;
+        if (S.role[s] == 1) {
+          push4(s, sub_node_first[s], 0, 5);
+          Q.nchunk_bwd[s] = 1;
+          continue;
+        }
+        Q.nchunk_bwd[s] = chunk_rows(s, 1, n, [n, m](int r) { return int64_t(n - r + m); });
       }
-      S.nchunk_fwdT[s] = chunk_rows(s, 2, n + m, [n](int c) { return c < n ? int64_t(c + 1) : int64_t(n); });
     }
-  }
-  for (int l = 0; l < S.nlevels; ++l) {
-    S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
-    for (int s : S.level_sups[l]) {
-      int n = S.n[s], m = S.m[s];
-      if (S.role[s] == 2) continue;
-      if (S.role[s] == 1) {
-        push4(s, sub_node_first[s], 0, 7);
-        S.nchunk_bwdT[s] = 1;
-        continue;
+    Q.phase_off.push_back(int32_t(Q.sitems.size() / 4));
+    Q.items_per_bin = Q.phase_off.back();
+    // transposed: fwdT levels deep->0 over output columns (n+m), bwdT levels 0->deep over n columns
+    int32_t base = Q.items_per_bin;
+    Q.phase_offT.clear();
+    for (int l = S.nlevels - 1; l >= 0; --l) {
+      Q.phase_offT.push_back(int32_t(Q.sitems.size() / 4) - base);
+      for (int s : S.level_sups[l]) {
+        int n = S.n[s], m = S.m[s];
+        if (S.role[s] == 2) continue;
+        if (S.role[s] == 1) {
+          push4(s, sub_node_first[s], 0, 6);
+          Q.nchunk_fwdT[s] = 1;
+          continue;
+        }
+        Q.nchunk_fwdT[s] = chunk_rows(s, 2, n + m, [n](int c) { return c < n ? int64_t(c + 1) : int64_t(n); });
       }
-      S.nchunk_bwdT[s] = chunk_rows(s, 3, n, [n, m](int c) { return int64_t(n - c + m); });
     }
+    for (int l = 0; l < S.nlevels; ++l) {
+      Q.phase_offT.push_back(int32_t(Q.sitems.size() / 4) - base);
+      for (int s : S.level_sups[l]) {
+        int n = S.n[s], m = S.m[s];
+        if (S.role[s] == 2) continue;
+        if (S.role[s] == 1) {
+          push4(s, sub_node_first[s], 0, 7);
+          Q.nchunk_bwdT[s] = 1;
+          continue;
+        }
+        Q.nchunk_bwdT[s] = chunk_rows(s, 3, n, [n, m](int c) { return int64_t(n - c + m); });
+      }
+    }
+    Q.phase_offT.push_back(int32_t(Q.sitems.size() / 4) - base);
+    Q.items_per_binT = Q.phase_offT.back();
   }
-  S.phase_offT.push_back(int32_t(S.sitems.size() / 4) - base);
-  S.items_per_binT = S.phase_offT.back();
   return std::string();
 }
 

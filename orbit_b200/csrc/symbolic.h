@@ -38,6 +38,20 @@ struct FactorLaunch {
   int64_t items;     // number of items (per instance)
 };
 
+// Solve schedule (per bin, shared by all instances): items {s, r0, r1, kind}
+// with kinds 0 fwd, 1 bwd, 2 fwdT, 3 bwdT (row chunks of one supernode) and
+// 4..7 the same sweeps over a whole subtree {root, first node, 0, kind}.
+struct SolveSched {
+  int chunk_elems = 0;
+  std::vector<int32_t> sitems;            // 4 ints per item
+  std::vector<int32_t> phase_off;         // non-transposed phases (2*nlevels+1 offsets)
+  std::vector<int32_t> phase_offT;        // transposed phases
+  int32_t items_per_bin = 0, items_per_binT = 0;
+  // per supernode number of chunks in each solve kind
+  std::vector<int32_t> nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT;
+};
+constexpr int kNumSched = 3;
+
 struct Symbolic {
   int nz = 0, ny = 0, nx = 0;
   int64_t N = 0;
@@ -76,15 +90,7 @@ struct Symbolic {
   // factorization schedule; items are int4 {a,b,c,d}
   std::vector<int32_t> fitems;            // 4 ints per item
   std::vector<FactorLaunch> fsched;
-  // solve schedule (per bin, shared by all instances): items {s, r0, r1, kind}
-  // kinds: 0 fwd, 1 bwd, 2 fwdT, 3 bwdT (row chunks of one supernode);
-  // 4..7 the same sweeps over a whole subtree {root, first node, 0, kind}
-  std::vector<int32_t> sitems;            // 4 ints per item
-  std::vector<int32_t> phase_off;         // non-transposed phases (2*nlevels+1 offsets)
-  std::vector<int32_t> phase_offT;        // transposed phases
-  int32_t items_per_bin = 0, items_per_binT = 0;
-  // per supernode number of chunks in each solve kind
-  std::vector<int32_t> nchunk_fwd, nchunk_bwd, nchunk_fwdT, nchunk_bwdT;
+  SolveSched sched[kNumSched];  // chunk/2, chunk, 2 chunk; sched[1] is the default
   std::vector<int32_t> role;  // 0 chunked node, 1 subtree-task root, 2 inside a subtree
   int max_front = 0;
   int max_sub_front = 0;  // largest n+m of a supernode inside a subtree task
