@@ -241,10 +241,10 @@ int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info) {
     return ORBIT_ERR_ARG;
   }
   const Symbolic& S = sym->S;
-  int64_t v[13] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
+  int64_t v[14] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
                    (int64_t)S.factor_flops, S.sched[1].items_per_bin, S.w_size, S.leaf_cells, S.max_nm,
-                   S.max_sub_front};
-  for (int i = 0; i < n_info && i < 13; ++i) info[i] = v[i];
+                   S.max_sub_front, S.tc_pack_size};
+  for (int i = 0; i < n_info && i < 14; ++i) info[i] = v[i];
   return ORBIT_OK;
 }
 
@@ -410,10 +410,26 @@ int orbit_factor_create_ex(orbit_symbolic_t sym, int n_orbits, int n_sets, int n
     return code;
   };
   // fronts: group size from a budget
-  const size_t budget = (size_t)8 << 30;
-  int64_t per_inst = 2 * S.front_buf_size * (int64_t)vb;
-  int64_t G = per_inst > 0 ? (int64_t)(budget / per_inst) : n_inst;
-  G = std::max<int64_t>(1, std::min<int64_t>(G, n_inst));
+  // Factorization scratch (two level buffers of fronts per instance, plus the
+  // tensor-core operand packs of fp32 factors) for a group of instances that
+  // is factored together: 32 GB or 15% of the device, whichever is smaller,
+  // with the instances split into groups of equal size.
+  size_t budget = (size_t)32 << 30;
+  {
+    int dev = 0;
+    size_t free_b = 0, total_b = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && total_b > 0)
+      budget = std::min(budget, total_b / 100 * 15);
+    else
+      cudaGetLastError();
+  }
+  if (const char* e = std::getenv("ORBIT_B200_FRONT_BUDGET_GB")) budget = (size_t)(std::atof(e) * (1 << 30));
+  const int64_t per_inst =
+      2 * S.front_buf_size * (int64_t)vb + (precision == ORBIT_PREC_FP32 ? S.tc_pack_size * 4 : 0);
+  int64_t G = per_inst > 0 ? std::max<int64_t>(1, (int64_t)(budget / per_inst)) : n_inst;
+  G = std::min<int64_t>(G, n_inst);
+  const int64_t ngroups = (n_inst + G - 1) / G;
+  G = (n_inst + ngroups - 1) / ngroups;
   f->front_group = (int)G;
   if ((rc = dalloc(A, reinterpret_cast<unsigned char**>(&f->factors), (size_t)n_inst * S.fac_size * vb))) return fail(rc);
   if ((rc = dalloc(A, reinterpret_cast<unsigned char**>(&f->fronts), (size_t)2 * G * S.front_buf_size * vb))) return fail(rc);

@@ -20,7 +20,7 @@ _INT64_ARRAYS = {"ginv_off", "uoff", "fac_off", "front_off", "level_front_size",
 
 INFO_KEYS = ("N", "nsuper", "nlevels", "factor_nnz", "factor_elems", "front_elems", "max_front",
              "factor_flops", "solve_items_per_bin", "update_len", "leaf_cells", "max_nm",
-             "max_sub_front")
+             "max_sub_front", "tc_pack_floats")
 
 
 class Symbolic:
@@ -31,8 +31,8 @@ class Symbolic:
         self._h = h
         self.nz, self.ny, self.nx = int(nz), int(ny), int(nx)
         self.N = self.nz * self.ny * self.nx
-        buf = (C.c_int64 * 13)()
-        _lib.check(L.orbit_symbolic_info(h, buf, 13))
+        buf = (C.c_int64 * len(INFO_KEYS))()
+        _lib.check(L.orbit_symbolic_info(h, buf, len(INFO_KEYS)))
         self.info = {k: int(buf[i]) for i, k in enumerate(INFO_KEYS)}
 
     @property
