@@ -242,10 +242,11 @@ __global__ void k_diag(FactorDev D, T* fronts, T* factors, int64_t i0, int p0, i
   const int ldf = D.ldf[s], ldn = D.ldn[s];
   T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += kThreads) {
-    int r = e / nb, c = e % nb;
-    Dm[r * kLdS + c] = F[(int64_t)(p0 + r) * ldf + p0 + c];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // element loops use a fixed 64-wide index space (no divisions by nb)
+  for (int e = tid; e < 64 * 64; e += kThreads) {
+    const int r = e >> 6, c = e & 63;
+    if (r < nb && c < nb) Dm[r * kLdS + c] = F[(int64_t)(p0 + r) * ldf + p0 + c];
   }
   __syncthreads();
   for (int k = 0; k < nb; ++k) {
@@ -254,22 +255,30 @@ __global__ void k_diag(FactorDev D, T* fronts, T* factors, int64_t i0, int p0, i
       raise_status(status, ORBIT_ERR_PIVOT);
     for (int i = k + 1 + tid; i < nb; i += kThreads) Dm[i * kLdS + k] /= piv;
     __syncthreads();
-    const int w = nb - k - 1;
-    for (int e = tid; e < w * w; e += kThreads) {
-      int i = k + 1 + e / w, j = k + 1 + e % w;
-      Dm[i * kLdS + j] -= Dm[i * kLdS + k] * Dm[k * kLdS + j];
+    for (int i = k + 1 + ty; i < nb; i += 16) {
+      const T l = Dm[i * kLdS + k];
+      for (int j = k + 1 + tx; j < nb; j += 16) Dm[i * kLdS + j] -= l * Dm[k * kLdS + j];
     }
     __syncthreads();
   }
+  // explicit inverses, one column per thread; four partial sums shorten the
+  // dependent chain of each entry
   if (tid < 64) {
     const int j = tid;
     if (j < nb) {
       for (int i = 0; i < j; ++i) Li[i * kLdS + j] = T(0);
       Li[j * kLdS + j] = T(1);
       for (int i = j + 1; i < nb; ++i) {
-        T acc = T(0);
-        for (int k = j; k < i; ++k) acc -= Dm[i * kLdS + k] * Li[k * kLdS + j];
-        Li[i * kLdS + j] = acc;
+        T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+        int k = j;
+        for (; k + 3 < i; k += 4) {
+          a0 -= Dm[i * kLdS + k] * Li[k * kLdS + j];
+          a1 -= Dm[i * kLdS + k + 1] * Li[(k + 1) * kLdS + j];
+          a2 -= Dm[i * kLdS + k + 2] * Li[(k + 2) * kLdS + j];
+          a3 -= Dm[i * kLdS + k + 3] * Li[(k + 3) * kLdS + j];
+        }
+        for (; k < i; ++k) a0 -= Dm[i * kLdS + k] * Li[k * kLdS + j];
+        Li[i * kLdS + j] = (a0 + a1) + (a2 + a3);
       }
     }
   } else if (tid < 128) {
@@ -278,17 +287,26 @@ __global__ void k_diag(FactorDev D, T* fronts, T* factors, int64_t i0, int p0, i
       for (int i = j + 1; i < nb; ++i) Ui[i * kLdS + j] = T(0);
       Ui[j * kLdS + j] = T(1) / Dm[j * kLdS + j];
       for (int i = j - 1; i >= 0; --i) {
-        T acc = T(0);
-        for (int k = i + 1; k <= j; ++k) acc += Dm[i * kLdS + k] * Ui[k * kLdS + j];
-        Ui[i * kLdS + j] = -acc / Dm[i * kLdS + i];
+        T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+        int k = i + 1;
+        for (; k + 3 <= j; k += 4) {
+          a0 += Dm[i * kLdS + k] * Ui[k * kLdS + j];
+          a1 += Dm[i * kLdS + k + 1] * Ui[(k + 1) * kLdS + j];
+          a2 += Dm[i * kLdS + k + 2] * Ui[(k + 2) * kLdS + j];
+          a3 += Dm[i * kLdS + k + 3] * Ui[(k + 3) * kLdS + j];
+        }
+        for (; k <= j; ++k) a0 += Dm[i * kLdS + k] * Ui[k * kLdS + j];
+        Ui[i * kLdS + j] = -((a0 + a1) + (a2 + a3)) / Dm[i * kLdS + i];
       }
     }
   }
   __syncthreads();
-  for (int e = tid; e < nb * nb; e += kThreads) {
-    int r = e / nb, c = e % nb;
-    F[(int64_t)(p0 + r) * ldf + p0 + c] = Dm[r * kLdS + c];
-    SQ[(int64_t)(p0 + r) * ldn + p0 + c] = r > c ? Li[r * kLdS + c] : Ui[r * kLdS + c];
+  for (int e = tid; e < 64 * 64; e += kThreads) {
+    const int r = e >> 6, c = e & 63;
+    if (r < nb && c < nb) {
+      F[(int64_t)(p0 + r) * ldf + p0 + c] = Dm[r * kLdS + c];
+      SQ[(int64_t)(p0 + r) * ldn + p0 + c] = r > c ? Li[r * kLdS + c] : Ui[r * kLdS + c];
+    }
   }
 }
 
