@@ -762,6 +762,17 @@ __global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, 
     // every issued copy has landed before this CTA may finish
     for (int kb = max(0, issued - kTcStages); kb < issued; ++kb)
       if (!tc::mbar_wait(&full[kb % kTcStages], (kb / kTcStages) & 1, kTcWaitLimit)) failed = 1;
+  } else if (job == 3 && warp >= 2) {
+    // the F22 tile this CTA updates does not depend on the GEMM: warps 2-3
+    // ask L2 for it while the main loop runs (one 128-byte line per request)
+    const int rows = min(128, M - tr * tc::kRows), cols = min(128, N - tcol * 128);
+    const float* C0 = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s] +
+                      (int64_t)(n + tr * tc::kRows) * ldf + n + tcol * 128;
+    for (int q = threadIdx.x - 64; q < rows * 5; q += 64) {
+      const int r = q / 5, seg = q - r * 5;
+      const float* a = C0 + (int64_t)r * ldf + min(seg * 32, cols - 1);  // stays inside the row
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+    }
   } else if (threadIdx.x == 32) {
     const uint32_t idesc = tc::idesc_tf32(128, 128);
     for (int kb = 0; kb < nk; ++kb) {
@@ -820,15 +831,14 @@ __global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, 
       const int col = cc * 32 + lane;
       if (col < cols) {
         if (job == 3) {
-          for (int r0 = 0; r0 < rows; r0 += 8) {
-            float c[8];
+          // all 32 rows' loads in flight before any update
+          float c[32];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-              if (r0 + u < rows) c[u] = C[(int64_t)(r0 + u) * ldc + col];
+          for (int u = 0; u < 32; ++u)
+            if (u < rows) c[u] = C[(int64_t)u * ldc + col];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-              if (r0 + u < rows) C[(int64_t)(r0 + u) * ldc + col] = c[u] + sw[(r0 + u) * 33 + lane];
-          }
+          for (int u = 0; u < 32; ++u)
+            if (u < rows) C[(int64_t)u * ldc + col] = c[u] + sw[u * 33 + lane];
         } else {
           const float sg = job == 0 ? 1.f : -1.f;
           for (int r = 0; r < rows; ++r) C[(int64_t)r * ldc + col] = sg * sw[r * 33 + lane];
