@@ -67,6 +67,7 @@ struct ChainDev {
   int total;
   long long spin_limit;
   int never_ready;  // self-test: the first task waits for a count nothing reaches
+  int prefetch;     // L2 prefetch of each task's factor rows before its dependency wait
 };
 
 __device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit) {
@@ -461,6 +462,32 @@ __global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(Chain
     const bool trans = kind == 2 || kind == 3 || kind == 6 || kind == 7;
     const bool subtree = kind >= 4;
     int* cbase = D.counters + (int64_t)o * 8 * 2 * D.nsuper;
+    // The factor rows of a row-chunk task do not depend on other tasks: ask L2
+    // for them before waiting (forward: whole rows of [SQ; Pb]; backward: the
+    // upper part of the SQ rows and the Qr rows), one request per 128 bytes.
+    // Off for FP64 at large batches, where the launch is throughput-bound and
+    // the requests only cost issue slots.
+    if (D.prefetch && (kind == 0 || kind == 1)) {
+      const int n_s = D.n[s], ldn_s = D.ldn[s];
+      const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+      constexpr int L = 128 / sizeof(T);
+      if (kind == 0) {
+        const char* a = reinterpret_cast<const char*>(SQ + (int64_t)it.y * ldn_s);
+        const int64_t bytes = (int64_t)(it.z - it.y) * ldn_s * sizeof(T);
+        for (int64_t q = (int64_t)tid * 128; q < bytes; q += (int64_t)kSolveThreads * 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a + q));
+      } else {
+        const int ldm_s = D.ldm[s], m_s = D.m[s];
+        const T* Qr = SQ + (int64_t)(n_s + m_s) * ldn_s;
+        for (int i = it.y + (tid >> 3); i < it.z; i += kSolveThreads / 8) {
+          const T* row = SQ + (int64_t)i * ldn_s;
+          for (int c = (i & ~(L - 1)) + (tid & 7) * L; c < n_s; c += 8 * L)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(row + c));
+          const T* qrow = Qr + (int64_t)i * ldm_s;
+          for (int c = (tid & 7) * L; c < m_s; c += 8 * L) asm volatile("prefetch.global.L2 [%0];" ::"l"(qrow + c));
+        }
+      }
+    }
     // ---- dependencies ----
     if (tid == 0) {
       bool ok = true;
@@ -568,6 +595,7 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.total = (tau1 - tau0) * D.items_per_bin * B;
   D.spin_limit = never_ready ? 20000LL : 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
   D.never_ready = never_ready ? 1 : 0;
+  D.prefetch = (sizeof(T) == 4 || B <= 6) ? 1 : 0;
   if (D.total <= 0) return ORBIT_OK;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->counters, 0, sizeof(int) * (size_t)f->n_orbits * 16 * S.nsuper, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
