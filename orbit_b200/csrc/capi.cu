@@ -412,14 +412,14 @@ int orbit_factor_create_ex(orbit_symbolic_t sym, int n_orbits, int n_sets, int n
   // fronts: group size from a budget
   // Factorization scratch (two level buffers of fronts per instance, plus the
   // tensor-core operand packs of fp32 factors) for a group of instances that
-  // is factored together: 32 GB or 15% of the device, whichever is smaller,
-  // with the instances split into groups of equal size.
-  size_t budget = (size_t)32 << 30;
+  // is factored together: 48 GB or a quarter of the device, whichever is
+  // smaller, with the instances split into groups of equal size.
+  size_t budget = (size_t)48 << 30;
   {
     int dev = 0;
     size_t free_b = 0, total_b = 0;
     if (cudaGetDevice(&dev) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && total_b > 0)
-      budget = std::min(budget, total_b / 100 * 15);
+      budget = std::min(budget, total_b / 4);
     else
       cudaGetLastError();
   }

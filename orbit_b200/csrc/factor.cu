@@ -628,20 +628,37 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
 
 static_assert(tc::kCols == kTcK && tc::kTileFloats == kTcTileFloats, "packed tile geometry");
 
-// Float offset of tile (t, kb) of a node's pack region: 0 = RA (mt x kt: F21,
-// later Pb), 1 = RB (mt x kt: F12^T), 2 = RC (nt x kt: inv(U11), later X),
-// 3 = RD (nt x kt: inv(L11)^T, later X^T).
+// Float offset of tile (t, kb) of a node's pack region (tiles of 2 x 2048
+// floats, hi then lo): 0 F21 (mt x kt), 1 F12^T (mt x kt), 2 inv(U11)
+// (nt x kt), 3 inv(L11)^T (nt x kt), 4 X (nt x kt), 5 X^T (nt x kt), 6 Pb
+// (mt x kt).  Regions 0-3 are written by k_tc_pack, 4-6 by GEMM epilogues.
 __device__ __forceinline__ int64_t tc_tile(int region, int t, int kb, int mt, int nt, int kt) {
+  const int64_t M = (int64_t)mt * kt, Nn = (int64_t)nt * kt;
   const int64_t base = region == 0   ? 0
-                       : region == 1 ? (int64_t)mt * kt
-                       : region == 2 ? 2LL * mt * kt
-                                     : 2LL * mt * kt + (int64_t)nt * kt;
+                       : region == 1 ? M
+                       : region == 2 ? 2 * M
+                       : region == 3 ? 2 * M + Nn
+                       : region == 4 ? 2 * M + 2 * Nn
+                       : region == 5 ? 2 * M + 3 * Nn
+                                     : 2 * M + 4 * Nn;
   return (base + (int64_t)t * kt + kb) * (2 * tc::kTileFloats);
 }
 
-// One 128 x 16 operand tile.  A-side operands (rows x K, read along rows):
-// op 0 F21, op 2 inv(U11), op 4 X, op 6 Pb.  B-side operands (columns x K,
-// read down columns): op 1 F12^T, op 3 inv(L11)^T (unit diagonal), op 5 X^T.
+// Split four values into tf32 hi/lo and store them as one 16-byte chunk of
+// the hi plane and of the lo plane.
+__device__ __forceinline__ void store_split4(float* tile, int off, float a, float b, float c, float d) {
+  float4 hi, lo;
+  hi.x = tc::to_tf32(a); lo.x = tc::to_tf32(a - hi.x);
+  hi.y = tc::to_tf32(b); lo.y = tc::to_tf32(b - hi.y);
+  hi.z = tc::to_tf32(c); lo.z = tc::to_tf32(c - hi.z);
+  hi.w = tc::to_tf32(d); lo.w = tc::to_tf32(d - hi.w);
+  *reinterpret_cast<float4*>(tile + off) = hi;
+  *reinterpret_cast<float4*>(tile + tc::kTileFloats + off) = lo;
+}
+
+// One 128 x 16 operand tile: op 0 F21 and op 2 inv(U11) (A side: rows x K,
+// read along rows), op 1 F12^T and op 3 inv(L11)^T with its unit diagonal
+// (B side: columns x K, read down columns).
 __global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* fronts, const float* factors,
                                                  float* pack, int64_t i0, int inst_base) {
   const int4 it = D.items[i0 + blockIdx.x];
@@ -650,9 +667,9 @@ __global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* front
   const int mt = (m + 127) / 128, nt = (n + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
   const float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   const float* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
-  const int region = (op == 0 || op == 6) ? 0 : op == 1 ? 1 : (op == 2 || op == 4) ? 2 : 3;
-  const int rows = (op == 0 || op == 1 || op == 6) ? m : n;
-  const bool bside = op == 1 || op == 3 || op == 5;
+  const int region = op;
+  const int rows = op <= 1 ? m : n;
+  const bool bside = op == 1 || op == 3;
   float* dst = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s] + tc_tile(region, t, kb, mt, nt, kt);
   for (int q = threadIdx.x; q < tc::kRows * (tc::kCols / 4); q += blockDim.x) {
     // A side: 4 consecutive threads read one 64-byte row segment; B side:
@@ -671,22 +688,12 @@ __global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* front
           case 0: x = F[(int64_t)(n + row) * ldf + kk]; break;
           case 1: x = F[(int64_t)kk * ldf + n + row]; break;
           case 2: x = kk >= row ? SQ[(int64_t)row * ldn + kk] : 0.f; break;
-          case 3: x = row < kk ? SQ[(int64_t)kk * ldn + row] : (row == kk ? 1.f : 0.f); break;
-          case 4: x = F[(int64_t)row * ldf + kk]; break;
-          case 5: x = F[(int64_t)kk * ldf + row]; break;
-          default: x = SQ[(int64_t)(n + row) * ldn + kk]; break;
+          default: x = row < kk ? SQ[(int64_t)kk * ldn + row] : (row == kk ? 1.f : 0.f); break;
         }
       }
       v[u] = x;
     }
-    float4 hi, lo;
-    hi.x = tc::to_tf32(v[0]); lo.x = tc::to_tf32(v[0] - hi.x);
-    hi.y = tc::to_tf32(v[1]); lo.y = tc::to_tf32(v[1] - hi.y);
-    hi.z = tc::to_tf32(v[2]); lo.z = tc::to_tf32(v[2] - hi.z);
-    hi.w = tc::to_tf32(v[3]); lo.w = tc::to_tf32(v[3] - hi.w);
-    const int o = tc::swz(r, c * 4);
-    *reinterpret_cast<float4*>(dst + o) = hi;
-    *reinterpret_cast<float4*>(dst + tc::kTileFloats + o) = lo;
+    store_split4(dst, tc::swz(r, c * 4), v[0], v[1], v[2], v[3]);
   }
 }
 
@@ -695,16 +702,16 @@ constexpr int kTcStageBytes = 4 * tc::kTileBytes;  // A hi, A lo, B hi, B lo
 constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 512;
 constexpr long long kTcWaitLimit = 1LL << 22;
 
-// One 128 x 128 output tile per CTA of job 0 (X, written over F11), 1 (Pb,
-// into the factor storage), 2 (Qr, into the factor storage) or 3 (F22 += Pb
-// F12).  Two CTAs per SM (96 KB ring and 128 TMEM columns each) so that one
+// One 128 x 128 output tile per CTA of job 0 (X, written only as the X and
+// X^T operand packs), 1 (Pb, into the factor storage and as the Pb operand
+// pack), 2 (Qr, into the factor storage) or 3 (F22 += Pb F12).  Two CTAs per SM (96 KB ring and 128 TMEM columns each) so that one
 // CTA's epilogue overlaps the other's main loop.  Warp 0 lane 0 streams the
 // k-blocks into a 3-stage ring, warp 1 lane 0 issues the MMAs, all four warps
 // read the accumulator back (warp w owns TMEM lanes 32w..32w+31 = tile rows)
 // and stage it through shared memory so that the output goes row by row,
 // coalesced.  Every wait is bounded; on a timeout the CTA lets its copies
 // land, skips the update, raises ORBIT_ERR_TIMEOUT and frees its tensor memory.
-__global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, float* factors, const float* pack,
+__global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, float* factors, float* pack,
                                                     int64_t i0, int inst_base, int* status) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t full[kTcStages], empty[kTcStages], done;
@@ -716,14 +723,15 @@ __global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, 
   const int s = it.x, tr = it.y, tcol = it.z, job = it.w;
   const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s], ldm = D.ldm[s];
   const int mt = (m + 127) / 128, nt = (n + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
-  const int ra = (job == 0 || job == 2) ? 2 : 0;
-  const int rb = (job == 0 || job == 1) ? 3 : 1;
+  const int ra = job == 0 ? 2 : job == 1 ? 0 : job == 2 ? 4 : 6;
+  const int rb = job == 0 ? 3 : job == 1 ? 5 : 1;
   const int M = (job == 0 || job == 2) ? n : m;
   const int N = (job == 0 || job == 1) ? n : m;
   // X = inv(U11) inv(L11): both factors vanish below k = max(row, column)
   const int kb0 = job == 0 ? (tc::kRows / tc::kCols) * max(tr, tcol) : 0;
   const int nk = kt - kb0;
-  const float* pk = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s];
+  float* pk2 = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s];
+  const float* pk = pk2;
   const float* pa = pk + tc_tile(ra, tr, kb0, mt, nt, kt);
   const float* pb = pk + tc_tile(rb, tcol, kb0, mt, nt, kt);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -801,11 +809,9 @@ __global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, 
   if (good) {
     float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
     float* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
-    float* C;
-    int ldc;
+    float* C = nullptr;
+    int ldc = 0;
     if (job == 0) {
-      C = F;
-      ldc = ldf;
     } else if (job == 1) {
       C = SQ + (int64_t)n * ldn;
       ldc = ldn;
@@ -820,14 +826,50 @@ __global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, 
     // blocks through a private padded buffer
     float* sw = reinterpret_cast<float*>(sbuf) + warp * 32 * 33;
     const int rows = min(32, M - tr * tc::kRows - warp * 32);
-    const int cols = min(128, N - tcol * 128);
-    C += (int64_t)(tr * tc::kRows + warp * 32) * ldc + tcol * 128;
-    for (int cc = 0; cc < 4 && cc * 32 < cols; ++cc) {
+    const int cols = job == 0 ? 0 : min(128, N - tcol * 128);
+    // operand packs written here cover the K extent of the next GEMMs
+    // (zero-padded rows and columns included: the accumulator is zero there)
+    const int kcols = job <= 1 ? min(128, tc::kCols * kt - 128 * tcol) : 0;
+    if (C) C += (int64_t)(tr * tc::kRows + warp * 32) * ldc + tcol * 128;
+    for (int cc = 0; cc < 4 && cc * 32 < max(cols, kcols); ++cc) {
       float v[32];
       tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
+      if (job <= 1) {
+        // A-side pack of this row block: X (job 0) or Pb = -acc (job 1)
+        const float sg = job == 0 ? 1.f : -1.f;
+        const int rl = warp * 32 + lane;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int kb = tcol * (tc::kRows / tc::kCols) + cc * 2 + h;
+          if (kb < kt) {
+            float* tile = pk2 + tc_tile(job == 0 ? 4 : 6, tr, kb, mt, nt, kt);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              store_split4(tile, tc::swz(rl, q * 4), sg * v[h * 16 + q * 4], sg * v[h * 16 + q * 4 + 1],
+                           sg * v[h * 16 + q * 4 + 2], sg * v[h * 16 + q * 4 + 3]);
+          }
+        }
+      }
 #pragma unroll
       for (int j = 0; j < 32; ++j) sw[lane * 33 + j] = v[j];
       __syncwarp();
+      if (job == 0) {
+        // B-side pack X^T: pack row = X column, K = X row
+        const int crow = cc * 32 + lane;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int kb = tr * (tc::kRows / tc::kCols) + warp * 2 + h;
+          if (kb < kt) {
+            float* tile = pk2 + tc_tile(5, tcol, kb, mt, nt, kt);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int r = h * 16 + q * 4;
+              store_split4(tile, tc::swz(crow, q * 4), sw[r * 33 + lane], sw[(r + 1) * 33 + lane],
+                           sw[(r + 2) * 33 + lane], sw[(r + 3) * 33 + lane]);
+            }
+          }
+        }
+      }
       const int col = cc * 32 + lane;
       if (col < cols) {
         if (job == 3) {

@@ -398,16 +398,17 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     // assembled): X = inv(U11) inv(L11); Pb = -F21 X; Qr = -X F12; then the
     // Schur complement F22 += Pb F12.  Each GEMM reads operands packed as tf32
     // hi/lo tiles; pack items are {s, op, tile, k-block}, GEMM items
-    // {s, row tile, column tile, job}.  Per node the pack holds regions
-    // RA (mt x kt tiles: F21, later Pb), RB (mt x kt: F12^T) and RC
-    // (2 x nt x kt: inv(U11) and inv(L11)^T, later X and X^T).
+    // {s, row tile, column tile, job}.  Per node the pack holds F21 and F12^T
+    // (mt x kt tiles each), inv(U11), inv(L11)^T, X and X^T (nt x kt each) and
+    // Pb (mt x kt); the X GEMM writes the X packs and the Pb GEMM the Pb pack
+    // from their epilogues.
     if (!big.empty()) {
       int64_t pack = 0;
       for (int s : big) {
         const int64_t mt = (S.m[s] + kSchurTile - 1) / kSchurTile, nt = (S.n[s] + kSchurTile - 1) / kSchurTile;
         const int64_t kt = (S.n[s] + kTcK - 1) / kTcK;
         S.tc_pack_off[s] = pack;
-        pack += (2 * mt + 2 * nt) * kt * 2 * kTcTileFloats;
+        pack += (3 * mt + 4 * nt) * kt * 2 * kTcTileFloats;
       }
       S.tc_pack_size = std::max(S.tc_pack_size, pack);
       auto pack_launch = [&](std::initializer_list<int> ops) {
@@ -436,10 +437,8 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
         S.fsched.push_back({FactorLaunch::TC_GEMM, l, 0, off, nitems() - off});
       };
       pack_launch({0, 1, 2, 3});  // F21, F12^T, inv(U11), inv(L11)^T
-      gemm_launch({0});           // X
-      pack_launch({4, 5});        // X, X^T
-      gemm_launch({1, 2});        // Pb, Qr
-      pack_launch({6});           // Pb
+      gemm_launch({0});           // X (and its packs)
+      gemm_launch({1, 2});        // Pb (and its pack), Qr
       gemm_launch({3});           // Schur complement
     }
   }

@@ -82,7 +82,7 @@ class _Entry:
         info = sym.info
         scratch = 2 * info["front_elems"] * vb + (info["tc_pack_floats"] * 4 if precision == 32 else 0)
         self.bytes = (self.n_species * N_BINS * (info["factor_elems"] * vb + 7 * sym.N * 8)
-                      + min(32 << 30, self.n_species * N_BINS * scratch)
+                      + min(48 << 30, self.n_species * N_BINS * scratch)
                       + slots * 60 * sym.N * 8)
 
     def build(self):
