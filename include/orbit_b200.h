@@ -85,6 +85,16 @@ typedef struct {
  * 299-335); like them it is computed once and reused for every species,
  * bin and met draw of the domain.  leaf_cells <= 0 selects the default. */
 int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out);
+/* orbit_symbolic_create with every tuning option explicit (the autotuner's
+ * search space): nested-dissection leaf size, solve chunk size (factor entries
+ * per row chunk of the medium-batch schedule; the small- and large-batch
+ * schedules use half and twice that), the smallest pivot count of a
+ * tensor-core supernode, and the whole-subtree solve-task divisor (0 = none).
+ * Values <= 0 (subtree_div < 0) take the ORBIT_B200_* environment setting or
+ * the default.  Extends the ordering options of umfpack_symbolic
+ * (orbit/core/solve.py:88-207: ordering, qinit). */
+int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_elems, int tc_min_n,
+                             int subtree_div, orbit_symbolic_t* out);
 /* Replaces umfpack_free_symbolic (orbit/core/solve.py:291-296). */
 int orbit_symbolic_destroy(orbit_symbolic_t sym);
 /* info[0..12] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor

@@ -43,6 +43,8 @@ EXPORTS = {
     "orbit_kernel_launches": (C.c_longlong, []),
     "orbit_factor_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "orbit_symbolic_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "orbit_symbolic_create_ex": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.POINTER(C.c_void_p)]),
     "orbit_symbolic_destroy": (C.c_int, [C.c_void_p]),
     "orbit_symbolic_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int]),
     "orbit_symbolic_perm": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -205,20 +205,27 @@ int orbit_factor_profile(orbit_factor_t f, int mode, double* out) {
   return ORBIT_OK;
 }
 
-int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out) {
+int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_elems, int tc_min_n,
+                             int subtree_div, orbit_symbolic_t* out) {
   if (!out) {
     set_last_error("out is NULL");
     return ORBIT_ERR_ARG;
   }
   *out = nullptr;
+  // unset options (<= 0; subtree_div < 0) take the environment's value, if
+  // any, else the built-in default
+  auto env_int = [](const char* name, int fallback) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : fallback;
+  };
+  SymbolicOptions opt;
+  opt.leaf_cells = leaf_cells > 0 ? leaf_cells : std::max(1, env_int("ORBIT_B200_LEAF", kDefaultLeaf));
+  opt.chunk_elems = std::max(256, chunk_elems > 0 ? chunk_elems : env_int("ORBIT_B200_CHUNK", kChunkElems));
+  opt.tc_min_n = std::max(1, tc_min_n > 0 ? tc_min_n : env_int("ORBIT_B200_TC_MIN_N", opt.tc_min_n));
+  opt.subtree_div = subtree_div >= 0 ? subtree_div : std::max(0, env_int("ORBIT_B200_SUBTREE_DIV", 0));
   orbit_symbolic_s* h = new (std::nothrow) orbit_symbolic_s();
   if (!h) return ORBIT_ERR_NOMEM;
-  int chunk = kChunkElems;
-  if (const char* e = std::getenv("ORBIT_B200_CHUNK")) chunk = std::max(256, std::atoi(e));
-  int leaf = leaf_cells > 0 ? leaf_cells : kDefaultLeaf;
-  if (leaf_cells <= 0)
-    if (const char* e = std::getenv("ORBIT_B200_LEAF")) leaf = std::max(1, std::atoi(e));
-  std::string err = build_symbolic(nz, ny, nx, leaf, chunk, h->S);
+  std::string err = build_symbolic(nz, ny, nx, opt, h->S);
   if (!err.empty()) {
     set_last_error(err);
     delete h;
@@ -226,6 +233,10 @@ int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic
   }
   *out = h;
   return ORBIT_OK;
+}
+
+int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic_t* out) {
+  return orbit_symbolic_create_ex(nz, ny, nx, leaf_cells, 0, 0, -1, out);
 }
 
 int orbit_symbolic_destroy(orbit_symbolic_t sym) {

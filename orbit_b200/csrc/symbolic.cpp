@@ -41,8 +41,9 @@ struct Node {
 
 }  // namespace
 
-std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_elems,
-                           Symbolic& S) {
+std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, Symbolic& S) {
+  int leaf_cells = opt.leaf_cells;
+  int chunk_elems = opt.chunk_elems;
   if (nz < 1 || ny < 1 || nx < 1) return "grid dimensions must be positive";
   if (int64_t(nz) * ny * nx > (int64_t(1) << 30)) return "grid too large";
   if (leaf_cells < 1) leaf_cells = 1;
@@ -279,8 +280,7 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
     }
 
   // ---- factorization schedule ----
-  S.tc_min_n = 48;
-  if (const char* e = std::getenv("ORBIT_B200_TC_MIN_N")) S.tc_min_n = std::max(1, std::atoi(e));
+  S.tc_min_n = std::max(1, opt.tc_min_n);
   S.tc_pack_off.assign(ns, -1);
   S.tc_pack_size = 0;
   auto push_item = [&](int a, int b, int c, int d) {
@@ -469,12 +469,8 @@ std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_ele
   }
   // Off by default: with several rows per warp in the chunked tasks, per-node
   // chunks beat whole-subtree tasks at every batch size measured (1 to 12
-  // orbits).  ORBIT_B200_SUBTREE_DIV=d enables them below fac_nnz / d work.
-  int64_t wmax = 0;
-  if (const char* e = std::getenv("ORBIT_B200_SUBTREE_DIV")) {
-    const int64_t div = std::atoll(e);
-    wmax = div > 0 ? std::max<int64_t>(1, S.fac_nnz / div) : 0;
-  }
+  // orbits).  subtree_div = d merges subtrees below fac_nnz / d work.
+  const int64_t wmax = opt.subtree_div > 0 ? std::max<int64_t>(1, S.fac_nnz / opt.subtree_div) : 0;
   // role: 0 = chunked node, 1 = subtree root, 2 = inside a subtree
   S.role.assign(ns, 0);
   for (int s = ns - 1; s >= 0; --s) {

@@ -104,9 +104,16 @@ struct Symbolic {
   int64_t tc_pack_size = 0;  // floats per instance (max over levels)
 };
 
+// Tuning options of the analysis (the autotuner's search space).
+struct SymbolicOptions {
+  int leaf_cells = 64;    // nested-dissection leaf size (cells)
+  int chunk_elems = 8192; // solve row-chunk size of the medium schedule (factor entries)
+  int tc_min_n = 48;      // smallest pivot count of a tensor-core supernode (fp32 factors)
+  int subtree_div = 0;    // > 0: whole-subtree solve tasks below fac_nnz / subtree_div; 0: none
+};
+
 // Build the symbolic analysis.  Returns an empty string on success, an
 // error message otherwise.
-std::string build_symbolic(int nz, int ny, int nx, int leaf_cells, int chunk_elems,
-                           Symbolic& S);
+std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, Symbolic& S);
 
 }  // namespace orbit

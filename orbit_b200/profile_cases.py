@@ -33,7 +33,7 @@ def main():
     mets = [device.MetDevice(g) for g in met]
     T = [device.assemble_transport(m) for m in mets]
     sinks = [torch.as_tensor(d, device="cuda") for s in spc for d in s.sink_diag(met)]
-    sym = Symbolic(nz, ny, nx)
+    sym = Symbolic.tuned(nz, ny, nx, args.precision, args.orbits)  # the bench's analysis options
     fb = device.FactorBatch(sym, args.orbits, args.precision)
     fb.numeric([T[t] for _ in range(args.orbits) for t in range(8)], sinks)
     if args.stage == "chain":
