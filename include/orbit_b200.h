@@ -143,6 +143,17 @@ int orbit_mass_balance_rows(int nz, int ny, int nx, int nbins, const double* con
 int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
                      const double* c, double dt, int limited, double* d, orbit_stream_t stream);
 
+/* Frozen-gain FCT tangent-linear operator L_AD of n_vec baseline
+ * concentrations c_base (device, n_vec x N): per face the gain C * beta of the
+ * baseline (Zalesak coefficient times van Leer reconstruction factor) over dx,
+ * terrain-weighted, in concentration form, so that L_AD c_base = -d_AD(c_base).
+ * Output: n_vec stencils in the 7-point layout of the transport blocks
+ * (device, n_vec x 7 x N doubles; the vertical entries are zero), so
+ * T + L_AD is a plain stencil sum that the factorization accepts.  Replaces
+ * assemble_fct_linear_operator (orbit/core/fct.py:495-572). */
+int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c_base,
+                              double dt, double* stencil, orbit_stream_t stream);
+
 /* K2 without device allocation, for callers that cannot allocate device
  * memory at the point where they apply the FCT correction (a host model that
  * owns its whole device-memory budget through its own pool, or a time loop

@@ -55,6 +55,8 @@ int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const 
                int limited, double* d, double* scratch, cudaStream_t st);
 int fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
                        double dt, int limited, double* d, cudaStream_t st);
+int fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
+                        double* stencil, double* scratch, cudaStream_t st);
 
 namespace {
 
@@ -365,6 +367,21 @@ int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, 
   double* scratch = nullptr;
   ORBIT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(double) * 3 * N * n_vec, st));
   int rc = fct_source(nz, ny, nx, met, n_vec, c, dt, limited, d, scratch, st);
+  cudaFreeAsync(scratch, st);
+  return rc;
+}
+
+int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c_base,
+                              double dt, double* stencil, orbit_stream_t stream) {
+  if (!met || !c_base || !stencil || n_vec < 1 || nz < 1 || ny < 1 || nx < 1 || !(dt > 0)) {
+    set_last_error("orbit_fct_linear_operator: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t N = (int64_t)nz * ny * nx;
+  double* scratch = nullptr;
+  ORBIT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(double) * 3 * N * n_vec, st));
+  int rc = fct_linear_operator(nz, ny, nx, met, n_vec, c_base, dt, stencil, scratch, st);
   cudaFreeAsync(scratch, st);
   return rc;
 }

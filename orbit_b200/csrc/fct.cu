@@ -47,7 +47,7 @@ __device__ __forceinline__ double dx_at(const orbit_met_t& g, int j) {
 // Face between lo = (k, j, i-1) [x] or (k, j-1, i) [y] and hi = cell index `hi`.
 // Returns flux = A * inv and the terrain weights; valid flag.
 struct Face {
-  double flux, trL, trR;
+  double flux, trL, trR, beta, inv;
   bool ok;
 };
 
@@ -76,6 +76,8 @@ __device__ Face x_face(const FctGeom& G, const double* x, int k, int j, int ihi)
   f.trL = f.ok ? face / (dl > 0.0 ? dl : 1.0) : 1.0;
   f.trR = f.ok ? face / (dr > 0.0 ? dr : 1.0) : 1.0;
   f.flux = A * inv;
+  f.beta = beta;
+  f.inv = inv;
   return f;
 }
 
@@ -105,6 +107,8 @@ __device__ Face y_face(const FctGeom& G, const double* x, int k, int jhi, int i)
   f.trL = f.ok ? (dxf / (dxs > 0.0 ? dxs : 1.0)) * (face / (ds > 0.0 ? ds : 1.0)) : 1.0;
   f.trR = f.ok ? (dxf / (dxn > 0.0 ? dxn : 1.0)) * (face / (dn > 0.0 ? dn : 1.0)) : 1.0;
   f.flux = A * inv;
+  f.beta = beta;
+  f.inv = inv;
   return f;
 }
 
@@ -201,6 +205,68 @@ __global__ void k_fct_div(FctGeom G, const double* x_all, const double* Rp_all, 
   d_all[(int64_t)blockIdx.y * N + cell] = d * rho_at(G.g, cell);
 }
 
+// Frozen-gain linearisation of the limited flux (assemble_fct_linear_operator,
+// orbit/core/fct.py:495-572): each face's gain w = C beta / dx (C the Zalesak
+// coefficient and beta the van Leer reconstruction factor of the baseline),
+// distributed with the terrain weights so that L_AD x = -div(w (x_R - x_L)),
+// then the similarity diag(rho) L diag(1/rho).  Output: the 7-point stencil
+// layout of the transport blocks (centre, W, E, S, N, below, above; the
+// vertical entries are zero), so L_low + L_AD is a plain stencil sum.
+__global__ void k_fct_linop(FctGeom G, const double* x_all, const double* Rp_all, const double* Rm_all,
+                            double* st_all, int64_t N) {
+  const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= N) return;
+  const double* x = x_all + (int64_t)blockIdx.y * N;
+  const double* Rp = Rp_all + (int64_t)blockIdx.y * N;
+  const double* Rm = Rm_all + (int64_t)blockIdx.y * N;
+  double* st = st_all + (int64_t)blockIdx.y * 7 * N;
+  const int nx = G.nx, ny = G.ny;
+  const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
+  auto gain = [&](const Face& f, int64_t lo, int64_t hi) {
+    if (!f.ok) return 0.0;
+    const double into_hi = f.trR * f.flux;
+    const double C = into_hi >= 0.0 ? fmin(Rp[hi], Rm[lo]) : fmin(Rm[hi], Rp[lo]);
+    return fmin(fmax(C, 0.0), 1.0) * f.beta * f.inv;
+  };
+  const double rp = rho_at(G.g, cell);
+  double cen = 0.0, w = 0.0, e = 0.0, s = 0.0, n = 0.0;
+  if (nx > 1) {
+    if (i > 0) {  // west face: this cell is its high side
+      const Face f = x_face(G, x, k, j, i);
+      const double wr = f.trR * gain(f, cell - 1, cell);
+      cen -= wr;
+      w = wr * rp / rho_at(G.g, cell - 1);
+    }
+    if (i < nx - 1) {  // east face: low side
+      const Face f = x_face(G, x, k, j, i + 1);
+      const double wl = f.trL * gain(f, cell, cell + 1);
+      cen -= wl;
+      e = wl * rp / rho_at(G.g, cell + 1);
+    }
+  }
+  if (ny > 1) {
+    if (j > 0) {
+      const Face f = y_face(G, x, k, j, i);
+      const double wr = f.trR * gain(f, cell - nx, cell);
+      cen -= wr;
+      s = wr * rp / rho_at(G.g, cell - nx);
+    }
+    if (j < ny - 1) {
+      const Face f = y_face(G, x, k, j + 1, i);
+      const double wl = f.trL * gain(f, cell, cell + nx);
+      cen -= wl;
+      n = wl * rp / rho_at(G.g, cell + nx);
+    }
+  }
+  st[cell] = cen;
+  st[N + cell] = w;
+  st[2 * N + cell] = e;
+  st[3 * N + cell] = s;
+  st[4 * N + cell] = n;
+  st[5 * N + cell] = 0.0;
+  st[6 * N + cell] = 0.0;
+}
+
 }  // namespace
 
 int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
@@ -216,6 +282,24 @@ int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const 
   if (limited) k_fct_ratio<<<g, 128, 0, st>>>(G, x, Rp, Rm, N);
   note_launch();
   k_fct_div<<<g, 128, 0, st>>>(G, x, Rp, Rm, limited, d, N);
+  note_launch();
+  ORBIT_CUDA_TRY(cudaGetLastError());
+  return ORBIT_OK;
+}
+
+int fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
+                        double* stencil, double* scratch, cudaStream_t st) {
+  const int64_t N = (int64_t)nz * ny * nx;
+  FctGeom G{*met, nz, ny, nx, dt};
+  double* x = scratch;
+  double* Rp = scratch + (int64_t)n_vec * N;
+  double* Rm = Rp + (int64_t)n_vec * N;
+  dim3 g((unsigned)((N + 127) / 128), n_vec);
+  k_fct_x<<<g, 128, 0, st>>>(G, c, x, N);
+  note_launch();
+  k_fct_ratio<<<g, 128, 0, st>>>(G, x, Rp, Rm, N);
+  note_launch();
+  k_fct_linop<<<g, 128, 0, st>>>(G, x, Rp, Rm, stencil, N);
   note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;

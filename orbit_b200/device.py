@@ -88,6 +88,16 @@ def fct_source(met: MetDevice, c: torch.Tensor, dt: float = DTAU, limited: bool 
     return d.reshape(c.shape)
 
 
+def fct_linear_operator(met: MetDevice, c_base: torch.Tensor, dt: float = DTAU) -> torch.Tensor:
+    """Frozen-gain FCT operator L_AD of one or more baseline concentrations, as
+    [7, N] stencils (vertical entries zero) in the transport blocks' layout."""
+    c2 = c_base.reshape(-1, met.N).contiguous()
+    out = torch.empty((c2.shape[0], 7, met.N), dtype=torch.float64, device=c2.device)
+    _lib.check(_lib.lib().orbit_fct_linear_operator(met.nz, met.ny, met.nx, C.byref(met.struct), c2.shape[0],
+                                                    _lib.ptr(c2), float(dt), _lib.ptr(out), _stream()))
+    return out[0] if c_base.dim() == 1 else out
+
+
 def mass_balance(mets: Sequence[MetDevice], stencils: Sequence[torch.Tensor]) -> dict:
     """K7 row sums on the device, then the same order statistics the reference
     reports (operator.py:598-652): median, p90, p99, max of the interior rows

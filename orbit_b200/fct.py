@@ -4,6 +4,10 @@
 runs the two-pass Zalesak-limited anti-diffusive source on the device (K2)
 and returns a host array like the reference.  ``fct_source_device`` keeps
 everything on the device for the deferred-correction loop.
+``assemble_fct_linear_operator(grid, indexer, c_baseline_flat, dt)``
+(fct.py:495-572) builds the frozen-gain operator L_AD on the device and
+returns it as the reference's CSC matrix; ``fct_linear_operator_device``
+keeps it as a 7-point stencil that adds to a transport stencil.
 """
 from __future__ import annotations
 
@@ -26,3 +30,18 @@ def compute_horizontal_fct_source(grid, indexer, c_flat, dt, limited=True, c_gho
     md = device.MetDevice(met_from_griddata(grid))
     c = torch.as_tensor(np.asarray(c_flat, dtype=np.float64), device="cuda")
     return device.fct_source(md, c, dt, limited).cpu().numpy()
+
+
+def fct_linear_operator_device(met_device, c_base, dt=DTAU):
+    from . import device
+    return device.fct_linear_operator(met_device, c_base, dt)
+
+
+def assemble_fct_linear_operator(grid, indexer, c_baseline_flat, dt):
+    import torch
+    from . import device
+    md = device.MetDevice(met_from_griddata(grid))
+    c = torch.as_tensor(np.asarray(c_baseline_flat, dtype=np.float64), device="cuda")
+    st = device.fct_linear_operator(md, c, dt).cpu().numpy()
+    nz, ny, nx = md.nz, md.ny, md.nx
+    return device.stencil_to_csr(st, nz, ny, nx).tocsc()

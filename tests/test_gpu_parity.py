@@ -74,6 +74,27 @@ def test_fct_source_matches_reference(dev):
         assert _rel(dd[q], ofct.fct_source(MET[0], cv, 10800.0)) < 1e-12
 
 
+def test_fct_linear_operator_matches_reference(dev):
+    """Frozen-gain L_AD (fct.py:495-572) against the reference's CSC (golden),
+    the oracle for other baselines, and L_AD c = -d_AD(c) by construction."""
+    import torch
+    device, mets, _, _ = dev
+    g = MET[0]
+    c = torch.as_tensor(Z["fct_c"], device="cuda")
+    st = device.fct_linear_operator(mets[0], c).cpu().numpy()
+    L = device.stencil_to_csr(st, g.nz, g.ny, g.nx)
+    ref = golden_io.csc(Z, "fct_L0_")
+    assert abs(L - ref).max() <= 1e-12 * abs(ref).max()
+    assert _rel(L @ Z["fct_c"], -Z["fct_d0"]) < 1e-11
+    cc = torch.stack([c, 3.0 * c.flip(0)])
+    sts = device.fct_linear_operator(mets[1], cc).cpu().numpy()
+    for q, cv in enumerate(cc.cpu().numpy()):
+        want = ofct.fct_linear_operator(MET[1], cv, 10800.0)
+        got = device.stencil_to_csr(sts[q], g.nz, g.ny, g.nx)
+        assert abs(got - want).max() <= 1e-12 * abs(want).max()
+    assert np.all(sts[:, 5:] == 0.0)  # horizontal only: vertical entries stay zero
+
+
 def _batch(dev, precision=64, n=1):
     from orbit_b200.symbolic import Symbolic
     device, mets, T, sinks = dev
