@@ -211,6 +211,7 @@ def main():
     ap.add_argument("--draws", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-shared", action="store_true")
     args = ap.parse_args()
     rank, world, local = _env()
     if args.impl == "reference":
@@ -364,6 +365,54 @@ def main():
                  "latency_ms_p99": float(np.percentile(times, 99))}
         del fb1
 
+    # ---- shared operator: 64 marginal right-hand sides and 64 adjoint receptors
+    # on one factor set (species 0, draw 0), FP32 factors, tol 1e-6 ----
+    shared = None
+    if not args.no_shared:
+        n_rhs, stol = 64, 1e-6
+        fbS = device.FactorBatch(sym, n_rhs, args.precision, n_sets=1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        T0 = [device.assemble_transport(m) for m in met_dev[0]]
+        a.record()
+        fbS.numeric(T0, [sinks_d[0][0][bb] for bb in range(8)])
+        b.record()
+        torch.cuda.synchronize()
+        t_fac = a.elapsed_time(b)
+        rng = np.random.default_rng(2027)
+        dE = np.zeros((n_rhs, 8, sym.N))
+        R = np.zeros((n_rhs, 8, sym.N))
+        e0 = emis_h[0].reshape(8, NZ, NY, NX)
+        for q in range(n_rhs):
+            j0, i0 = rng.integers(0, NY - 5), rng.integers(0, NX - 5)
+            scale = np.exp(rng.normal(0.0, 0.1)) - 1.0  # +-10 % lognormal scaling of the patch
+            d = np.zeros((8, NZ, NY, NX))
+            d[:, 0, j0:j0 + 5, i0:i0 + 5] = scale * e0[:, 0, j0:j0 + 5, i0:i0 + 5]
+            dE[q] = d.reshape(8, -1)
+            j1, i1 = rng.integers(0, NY - 5), rng.integers(0, NX - 5)
+            r = np.zeros((8, NZ, NY, NX))
+            r[:, 0, j1:j1 + 5, i1:i1 + 5] = 1.0 / (8 * 25)  # receptor: mean over a surface patch
+            R[q] = r.reshape(8, -1)
+        dE_d = torch.as_tensor(dE, device="cuda")
+        R_d = torch.as_tensor(R, device="cuda")
+        fbS.solve(dE_d, tol=stol)
+        fbS.solve_adjoint(R_d, tol=stol)
+        barrier()
+        a.record()
+        _, inf_f = fbS.solve(dE_d, tol=stol)
+        b.record()
+        barrier()
+        t_f = a.elapsed_time(b)
+        a.record()
+        _, inf_a = fbS.solve_adjoint(R_d, tol=stol)
+        b.record()
+        barrier()
+        t_a = a.elapsed_time(b)
+        shared = {"rhs": n_rhs, "tol": stol, "factor_ms": t_fac,
+                  "forward_orbits_per_s": 1e3 * n_rhs / t_f, "adjoint_orbits_per_s": 1e3 * n_rhs / t_a,
+                  "forward_ms": t_f, "adjoint_ms": t_a,
+                  "all_converged": bool(np.all(inf_f[:, 4] > 0) and np.all(inf_a[:, 4] > 0))}
+        del fbS
+
     # ---- roofline of the chained-solve kernel (K4) ----
     peak, peak_kind = _peaks()
     chain_ms_avg = prof["chain_ms"] / max(prof["chain_launches"], 1)
@@ -406,6 +455,7 @@ def main():
             "latency_ms": {"batch_p50": float(np.percentile(lat_ms, 50)),
                            "batch_p99": float(np.percentile(lat_ms, 99))},
             "plain_fp64": plain,
+            "shared_operator": shared,
             "mixed_vs_plain": (value / world / plain["value"]) if plain else None,
             "max_rel_err_vs_fp64": err,
             "gmres_iters_median": float(np.median(it)) if it else None,

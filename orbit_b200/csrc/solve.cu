@@ -64,6 +64,7 @@ struct ChainDev {
   const int* set_of;  // factor set of each solve slot
   int n_bins;
   int B, tau0, tau1, trans;
+  int Borb;  // multi-RHS kernel: right-hand sides in the launch (B counts their groups)
   int total;
   long long spin_limit;
   int never_ready;  // self-test: the first task waits for a count nothing reaches
@@ -548,6 +549,221 @@ __global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(Chain
   }
 }
 
+// ---- many right-hand sides on one factor set ----
+//
+// When every solve slot of a handle maps onto the same factor set (marginal
+// perturbations or adjoint receptors of one operator), each task serves a
+// group of K right-hand sides: one claim, one dependency wait (on the group's
+// counters) and one barrier sequence, and every factor row loaded once is
+// multiplied against the K gathered vectors.  Non-transposed sweeps only.
+
+template <typename T, int G, int K>
+__device__ __forceinline__ void dot_seg_multi(const T* __restrict__ a, const T* v, int vcap, int nk, int j0, int j1,
+                                              int gl, T (&acc)[K]) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::w;
+  const int ja = min((j0 + W - 1) / W * W, j1);
+  const int jb = max(ja, j1 / W * W);
+  for (int j = j0 + gl; j < ja; j += G) {
+    const T x = __ldg(a + j);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) acc[k] = fma(x, v[k * vcap + j], acc[k]);
+  }
+  const V* a4 = reinterpret_cast<const V*>(a);
+  const int nv0 = ja / W, nv1 = jb / W;
+  for (int kk = nv0 + gl; kk < nv1; kk += 2 * G) {
+    const bool b1 = kk + G < nv1;
+    V x1 = {};
+    const V x0 = __ldg(a4 + kk);
+    if (b1) x1 = __ldg(a4 + kk + G);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) {
+        acc[k] += dot16(x0, v + k * vcap + kk * W);
+        if (b1) acc[k] += dot16(x1, v + k * vcap + (kk + G) * W);
+      }
+  }
+  for (int j = jb + gl; j < j1; j += G) {
+    const T x = __ldg(a + j);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) acc[k] = fma(x, v[k * vcap + j], acc[k]);
+  }
+}
+
+template <int G, int K, typename T, typename P, typename S>
+__device__ __forceinline__ void grouped_rows_multi(int r0, int r1, int wid, int nw, P&& partial, S&& store) {
+  constexpr int R = 32 / G;
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1), gr = lane / G;
+  for (int i0 = r0 + wid * R; i0 < r1; i0 += nw * R) {
+    const int i = i0 + gr;
+    T acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = T(0);
+    if (i < r1) partial(std::integral_constant<int, G>(), i, gl, acc);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (i < r1 && gl == 0) store(i, acc);
+  }
+}
+
+#define ORBIT_GROUPED_ROWS_MULTI(T, K, G_, r0, r1, wid, nw, partial, store)            \
+  do {                                                                                \
+    switch (G_) {                                                                     \
+      case 4: grouped_rows_multi<4, K, T>(r0, r1, wid, nw, partial, store); break;    \
+      case 8: grouped_rows_multi<8, K, T>(r0, r1, wid, nw, partial, store); break;    \
+      case 16: grouped_rows_multi<16, K, T>(r0, r1, wid, nw, partial, store); break;  \
+      default: grouped_rows_multi<32, K, T>(r0, r1, wid, nw, partial, store); break;  \
+    }                                                                                 \
+  } while (0)
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain_multi(ChainDev<T> D, int vcap) {
+  extern __shared__ unsigned char smem_raw[];
+  T* vbuf = reinterpret_cast<T*>(smem_raw);  // K vectors of vcap
+  __shared__ int s_task;
+  __shared__ int s_ok;
+  __shared__ int s_phase[kMaxPhases + 1];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int per_bin = D.items_per_bin * D.B;
+  for (int i = tid; i <= D.nphase; i += blockDim.x) s_phase[i] = D.phase_off[i] * D.B;
+  for (;;) {
+    if (tid == 0) {
+      s_task = atomicAdd(D.task_counter, 1);
+      s_ok = ld_volatile(D.status) == 0;
+    }
+    __syncthreads();
+    const int t = s_task;
+    if (t >= D.total || !s_ok) break;
+    const int q = t / per_bin;
+    const int r = t - q * per_bin;
+    const int tau = D.tau0 + q;
+    int lo = 0, hi = D.nphase;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_phase[mid] <= r) lo = mid;
+      else hi = mid;
+    }
+    const int rr = r - s_phase[lo];
+    const int cnt = D.phase_off[lo + 1] - D.phase_off[lo];
+    const int gi = rr / cnt;
+    const int4 it = D.items[D.phase_off[lo] + (rr - gi * cnt)];
+    const int s = it.x, kind = it.w, r0 = it.y, r1 = it.z;
+    const int nk = min(K, D.Borb - gi * K);
+    int o[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = D.orbit_ids[gi * K + (k < nk ? k : 0)];
+    int* cbase = D.counters + (int64_t)o[0] * 8 * 2 * D.nsuper;  // the group's counters
+    const int n = D.n[s], m = D.m[s], first = D.first[s], ldn = D.ldn[s], ldm = D.ldm[s];
+    const T* SQ = D.factors + ((int64_t)D.set_of[o[0]] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+    if (D.prefetch) {
+      if (kind == 0) {
+        const char* a = reinterpret_cast<const char*>(SQ + (int64_t)r0 * ldn);
+        const int64_t bytes = (int64_t)(r1 - r0) * ldn * sizeof(T);
+        for (int64_t q2 = (int64_t)tid * 128; q2 < bytes; q2 += (int64_t)kSolveThreads * 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a + q2));
+      }
+    }
+    if (tid == 0) {
+      bool ok = true;
+      if (kind == 0) {
+        for (int q2 = 0; q2 < 2 && ok; ++q2) {
+          const int c = D.child[2 * s + q2];
+          if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
+        }
+        if (ok && tau > D.tau0)
+          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+      } else {
+        const int par = D.parent[s];
+        if (par < 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit);
+        else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
+      }
+      s_ok = ok;
+      __threadfence();
+    }
+    __syncthreads();
+    if (!s_ok) break;
+    const int n0pad = (n + 3) & ~3;
+    if (kind == 0) {
+      // gather each right-hand side's vector over the range the rows read
+      const int lo_end = min(r1, n), hi0 = max(r0, n), w = n + m;
+      const int32_t* g0 = D.ginv + D.ginv_off[s];
+      const int32_t* g1 = g0 + w;
+      const int c0 = D.child[2 * s], c1 = D.child[2 * s + 1];
+      for (int k = 0; k < nk; ++k) {
+        T* vec = vbuf + k * vcap;
+        const double* Xin = D.X + ((int64_t)o[k] * 9 + tau) * D.N;
+        const double* Ein = D.E ? D.E + ((int64_t)o[k] * 8 + tau) * D.N : nullptr;
+        const double* Wo = D.W + (int64_t)o[k] * D.w_size;
+        const double* W0 = c0 >= 0 ? Wo + D.woff[c0] : nullptr;
+        const double* W1 = c1 >= 0 ? Wo + D.woff[c1] : nullptr;
+        for (int i = tid; i < lo_end; i += kSolveThreads) {
+          double v = Xin[first + i];
+          if (Ein) v += D.escale * Ein[first + i];
+          const int u0 = g0[i], u1 = g1[i];
+          if (u0 >= 0) v += W0[u0];
+          if (u1 >= 0) v += W1[u1];
+          vec[i] = (T)v;
+        }
+        for (int i = hi0 + tid; i < r1; i += kSolveThreads) {
+          double v = 0.0;
+          const int u0 = g0[i], u1 = g1[i];
+          if (u0 >= 0) v += W0[u0];
+          if (u1 >= 0) v += W1[u1];
+          vec[i] = (T)v;
+        }
+      }
+      __syncthreads();
+      const int64_t woff = D.woff[s];
+      auto partial = [&](auto g, int i, int gl, T(&acc)[K]) {
+        dot_seg_multi<T, decltype(g)::value, K>(SQ + (int64_t)i * ldn, vbuf, vcap, nk, 0, i < n ? i : n, gl, acc);
+      };
+      auto store = [&](int i, T(&acc)[K]) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (k < nk) {
+            const double y = (double)(vbuf[k * vcap + i] + acc[k]);
+            if (i < n) D.Y[(int64_t)o[k] * D.N + first + i] = y;
+            else D.W[(int64_t)o[k] * D.w_size + woff + (i - n)] = y;
+          }
+      };
+      const int Gl = group_lanes<T>(min(r1 - 1, n));
+      ORBIT_GROUPED_ROWS_MULTI(T, K, Gl, r0, r1, warp, kWarps, partial, store);
+    } else {
+      const int32_t* ui = D.uidx + D.uoff[s];
+      for (int k = 0; k < nk; ++k) {
+        T* vec = vbuf + k * vcap;
+        const double* Yo = D.Y + (int64_t)o[k] * D.N;
+        const double* Xout = D.X + ((int64_t)o[k] * 9 + tau + 1) * D.N;
+        for (int i = r0 + tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
+        for (int u = tid; u < m; u += kSolveThreads) vec[n0pad + u] = (T)Xout[ui[u]];
+      }
+      __syncthreads();
+      const T* Qr = SQ + (int64_t)(n + m) * ldn;
+      auto partial = [&](auto g, int i, int gl, T(&acc)[K]) {
+        constexpr int Gv = decltype(g)::value;
+        dot_seg_multi<T, Gv, K>(SQ + (int64_t)i * ldn, vbuf, vcap, nk, i, n, gl, acc);
+        dot_seg_multi<T, Gv, K>(Qr + (int64_t)i * ldm, vbuf + n0pad, vcap, nk, 0, m, gl, acc);
+      };
+      auto store = [&](int i, T(&acc)[K]) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (k < nk) D.X[((int64_t)o[k] * 9 + tau + 1) * D.N + first + i] = (double)acc[k];
+      };
+      const int Gl = group_lanes<T>(n - r0 + m);
+      ORBIT_GROUPED_ROWS_MULTI(T, K, Gl, r0, r1, warp, kWarps, partial, store);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      red_release_add(cbase + (tau * 2 + (kind == 0 ? 0 : 1)) * D.nsuper + s, 1);
+    }
+  }
+}
+
 // x[tau0] += escale * E[tau0] (forcing of the transposed chain's last bin)
 __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, int64_t N, int tau0,
                               double escale) {
@@ -567,9 +783,14 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.first = sy->d.first; D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent;
   D.child = sy->d.child; D.uidx = sy->d.uidx; D.rel = sy->d.rel; D.ldn = sy->d.ldn; D.ldm = sy->d.ldm;
   D.ginv = sy->d.ginv; D.ginv_off = sy->d.ginv_off;
+  // Right-hand sides on one factor set go through the multi-RHS kernel in
+  // groups of K (non-transposed sweeps of row-chunk tasks).
+  constexpr int KM = sizeof(T) == 4 ? 4 : 2;
+  const bool multi = !trans && !never_ready && f->n_sets == 1 && B >= 2 && S.max_sub_front == 0;
+  const int Bt = multi ? (B + KM - 1) / KM : B;  // task groups per (node chunk, bin)
   // schedule by batch size: small chunks shorten one orbit's critical path,
   // large ones cut per-task overhead when many orbits fill the GPU
-  const int ks = B <= 2 ? 0 : B <= 6 ? 1 : 2;
+  const int ks = Bt <= 2 ? 0 : Bt <= 6 ? 1 : 2;
   const SolveSched& Q = S.sched[ks];
   const auto& q = sy->d.sched[ks];
   D.nch_f = trans ? q.nchunk_fwdT : q.nchunk_fwd;
@@ -590,9 +811,9 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.factors = reinterpret_cast<const T*>(f->factors);
   D.X = X; D.E = E; D.escale = escale; D.Y = f->Ybuf; D.W = f->Wbuf;
   D.counters = f->counters; D.task_counter = f->task_counter; D.status = f->status;
-  D.orbit_ids = d_orbit_ids; D.B = B; D.tau0 = tau0; D.tau1 = tau1; D.trans = trans;
+  D.orbit_ids = d_orbit_ids; D.B = Bt; D.Borb = B; D.tau0 = tau0; D.tau1 = tau1; D.trans = trans;
   D.set_of = f->set_of; D.n_bins = f->n_bins;
-  D.total = (tau1 - tau0) * D.items_per_bin * B;
+  D.total = (tau1 - tau0) * D.items_per_bin * Bt;
   D.spin_limit = never_ready ? 20000LL : 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
   D.never_ready = never_ready ? 1 : 0;
   D.prefetch = (sizeof(T) == 4 || B <= 6) ? 1 : 0;
@@ -608,6 +829,36 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   int dev = 0, sms = 0, occ = 0;
   ORBIT_CUDA_TRY(cudaGetDevice(&dev));
   ORBIT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (multi) {
+    const int vcap = (S.max_front + 8 + 3) & ~3;
+    const size_t msmem = sizeof(T) * (size_t)KM * vcap;
+    {
+      int r0 = allow_max_smem((const void*)k_chain_multi<T, KM>);
+      if (r0) return r0;
+    }
+    ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_chain_multi<T, KM>, kSolveThreads, msmem));
+    if (occ < 1) {
+      set_last_error("chain kernel cannot be resident");
+      return ORBIT_ERR_INTERNAL;
+    }
+    int grid = sms * occ;
+    if (grid > D.total) grid = D.total;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (f->prof_on) {
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0, st);
+    }
+    k_chain_multi<T, KM><<<grid, kSolveThreads, msmem, st>>>(D, vcap);
+    note_launch();
+    if (f->prof_on) {
+      cudaEventRecord(e1, st);
+      f->prof_chain.push_back({e0, e1});
+      f->prof_chain_bytes += (double)B * (tau1 - tau0) * S.fac_nnz * sizeof(T);
+    }
+    ORBIT_CUDA_TRY(cudaGetLastError());
+    return ORBIT_OK;
+  }
   ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_chain<T>, kSolveThreads, smem));
   if (occ < 1) {
     set_last_error("chain kernel cannot be resident");
