@@ -154,6 +154,14 @@ int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
 int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c_base,
                               double dt, double* stencil, orbit_stream_t stream);
 
+/* y_v = beta y_v + alpha S_v x_v, or S_v^T x_v when trans, for n_vec 7-point
+ * stencils (device, n_vec x 7 x N) and vectors (device, n_vec x N): the
+ * products L_AD c_{tau+1} of the marginal FCT outer iteration and their
+ * transposes (orbit/modes/marginal.py:627-635, orbit/modes/adjoint.py:540-566
+ * apply the same operators as scipy CSC products). */
+int orbit_stencil_apply(int nz, int ny, int nx, int n_vec, const double* stencils, const double* x, double alpha,
+                        double beta, int trans, double* y, orbit_stream_t stream);
+
 /* K2 without device allocation, for callers that cannot allocate device
  * memory at the point where they apply the FCT correction (a host model that
  * owns its whole device-memory budget through its own pool, or a time loop

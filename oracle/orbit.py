@@ -13,6 +13,7 @@ reference's documented no-UMFPACK path (SciPy SuperLU, COLAMD):
 * ``solve_orbit_adjoint_one_species``         orbit/core/orbit_adjoint.py:70-144
 * ``gradient_per_emission_bin``               orbit/core/orbit_adjoint.py:147-153
 * the FCT deferred-correction schedule        orbit/cli.py:1204-1241
+* the marginal FCT outer GMRES                orbit/modes/marginal.py:627-720
 """
 from __future__ import annotations
 
@@ -142,3 +143,39 @@ def fct_deferred_solve(lus, e_list, met, passes, tol=1e-8, maxiter=200, dtau=DTA
         orbit, info = solve_orbit_one_species(lus, rhs, dtau, orbit[0], tol, maxiter)
         infos.append(info)
     return orbit, infos
+
+
+def fct_outer_solve(lus_per_orbit, e_lists, L_AD, tol=1e-8, rel_tol=2e-3, max_iters=40, dtau=DTAU):
+    """Marginal FCT outer solve (orbit/modes/marginal.py:627-720): the deferred
+    correction delta_c = K delta_c + b, b the low-order solution of the forcing,
+    K v the orbit of the extra right-hand sides -L_AD[o][tau] v[o][tau+1], solved
+    as GMRES on (I - K) delta_c = b over all orbits flattened (x0 = b,
+    atol = 0.3 rel_tol ||b||, restart min(max_iters, 30)), then one final pass
+    at the solution.  Returns (orbits per orbit as 9 arrays, outer iterations,
+    rel_final = max|g(x) - x| / max|g(x)|)."""
+    n = len(lus_per_orbit)
+    N = lus_per_orbit[0][0].shape[0]
+
+    def inner(extra):
+        out = []
+        for o in range(n):
+            e = [e_lists[o][t] + (extra[o][t] if extra is not None else 0.0) for t in range(N_BINS)]
+            orb, _ = solve_orbit_one_species(lus_per_orbit[o], e, dtau=dtau, tol=tol)
+            out.append(np.concatenate(orb))
+        return np.concatenate(out)
+
+    def extra_of(v):
+        vv = v.reshape(n, N_BINS + 1, N)
+        return [[-(L_AD[o][t] @ vv[o][t + 1]) for t in range(N_BINS)] for o in range(n)]
+
+    b = inner(None)
+    op = spla.LinearOperator((b.size, b.size), matvec=lambda v: v - (inner(extra_of(v)) - b), dtype=np.float64)
+    restart = min(max_iters, 30)
+    hist = []
+    x, _ = spla.gmres(op, b, x0=b.copy(), rtol=1e-30, atol=0.3 * rel_tol * np.linalg.norm(b), restart=restart,
+                      maxiter=max(1, -(-max_iters // restart)), callback=lambda r: hist.append(r),
+                      callback_type="pr_norm")
+    g = inner(extra_of(x))
+    rel = float(np.abs(g - x).max() / max(np.abs(g).max(), 1e-30))
+    orbits = [list(v) for v in g.reshape(n, N_BINS + 1, N)]
+    return orbits, len(hist), rel

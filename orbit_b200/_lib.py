@@ -58,6 +58,8 @@ EXPORTS = {
                                    C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_fct_linear_operator": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_double,
                                             C.c_void_p, C.c_void_p]),
+    "orbit_stencil_apply": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_fct_source_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_int,
                                            C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_factor_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

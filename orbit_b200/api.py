@@ -105,3 +105,95 @@ def solve_shared_operator(sym: Symbolic, T_stencils: Sequence[torch.Tensor], sin
     if adjoint:
         return fb.solve_adjoint(forcing, tol=tol, maxiter=maxiter)
     return fb.solve(forcing, tol=tol, maxiter=maxiter, dtau=dtau)
+
+
+def fct_operators(mets: Sequence["device.MetDevice"], c_base: torch.Tensor, dtau: float = DTAU) -> torch.Tensor:
+    """Frozen-gain L_AD of every bin at the baseline orbits' end-of-bin
+    concentrations (the marginal convention, marginal.py:627-635): (n, 8, 7, N)."""
+    n, N = c_base.shape[0], c_base.shape[-1]
+    L = torch.empty((n, N_BINS, 7, N), dtype=torch.float64, device=c_base.device)
+    for t in range(N_BINS):
+        L[:, t] = device.fct_linear_operator(mets[t], c_base[:, t + 1].contiguous(), dtau).reshape(n, 7, N)
+    return L
+
+
+def solve_marginal_fct(fb: "device.FactorBatch", mets: Sequence["device.MetDevice"], L_AD: torch.Tensor,
+                       E: torch.Tensor, tol: float = 1e-6, rel_tol: float = 2e-3, max_iters: int = 40,
+                       maxiter: int = 200, dtau: float = DTAU):
+    """Marginal FCT outer solve (marginal.py:627-720) for a batch of orbits on
+    the device.  The deferred correction delta_c = K delta_c + b (b the orbit of
+    the forcing E, K v the orbit of the extra right-hand sides
+    -L_AD[o][tau] v[o][tau+1]) is solved as restarted GMRES on (I - K) delta_c
+    = b over the whole batch (x0 = b, atol = 0.3 rel_tol ||b||, restart
+    min(max_iters, 30)); every application of K is one batched device solve of
+    all orbits.  A last pass at the solution returns consistent orbits.
+    Returns (orbits (n, 9, N), info dict)."""
+    n, N = E.shape[0], E.shape[-1]
+    g0 = mets[0]
+    nz, ny, nx = g0.nz, g0.ny, g0.nx
+    solves = [0]
+
+    def inner(extra):
+        orb, _ = fb.solve(E if extra is None else E + extra, tol=tol, maxiter=maxiter, dtau=dtau)
+        solves[0] += 1
+        return orb.reshape(-1)
+
+    def extra_of(v):
+        vv = v.reshape(n, N_BINS + 1, N)
+        ex = torch.empty((n, N_BINS, N), dtype=torch.float64, device=E.device)
+        for t in range(N_BINS):
+            ex[:, t] = device.stencil_apply(nz, ny, nx, L_AD[:, t], vv[:, t + 1].contiguous(), alpha=-1.0)
+        return ex
+
+    b = inner(None)
+    bnorm = float(torch.linalg.norm(b))
+    atol = 0.3 * rel_tol * bnorm
+    restart = min(max_iters, 30)
+
+    def matvec(v):
+        return v - (inner(extra_of(v)) - b)
+
+    x = b.clone()
+    iters, converged = 0, bnorm == 0.0
+    while not converged and iters < max_iters:
+        r = b - matvec(x)
+        beta = float(torch.linalg.norm(r))
+        if beta <= atol:
+            converged = True
+            break
+        V = [r / beta]
+        H = np.zeros((restart + 1, restart))
+        cs, sn = np.zeros(restart), np.zeros(restart)
+        gvec = np.zeros(restart + 1)
+        gvec[0] = beta
+        j = 0
+        for j in range(min(restart, max_iters - iters)):
+            w = matvec(V[j])
+            for i in range(j + 1):  # modified Gram-Schmidt
+                H[i, j] = float(torch.dot(w, V[i]))
+                w = w - H[i, j] * V[i]
+            H[j + 1, j] = float(torch.linalg.norm(w))
+            V.append(w / H[j + 1, j] if H[j + 1, j] > 0 else w)
+            for i in range(j):
+                t0 = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                H[i, j] = t0
+            den = np.hypot(H[j, j], H[j + 1, j])
+            cs[j], sn[j] = (H[j, j] / den, H[j + 1, j] / den) if den > 0 else (1.0, 0.0)
+            H[j, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j]
+            H[j + 1, j] = 0.0
+            gvec[j + 1] = -sn[j] * gvec[j]
+            gvec[j] = cs[j] * gvec[j]
+            iters += 1
+            if abs(gvec[j + 1]) <= atol:
+                break
+        k = j + 1
+        y = np.linalg.solve(np.triu(H[:k, :k]), gvec[:k])
+        for i in range(k):
+            x = x + float(y[i]) * V[i]
+        if abs(gvec[k]) <= atol:
+            converged = True
+    g = inner(extra_of(x))
+    rel_final = float((g - x).abs().max() / max(float(g.abs().max()), 1e-30))
+    info = {"outer_iters": iters, "inner_solves": solves[0], "rel_final": rel_final, "converged": converged}
+    return g.reshape(n, N_BINS + 1, N), info

@@ -264,7 +264,47 @@ __global__ void k_mass_rows(int nz, int ny, int nx, const double* const* Tst, co
   }
 }
 
+// y_v = beta y_v + alpha S_v x_v (or S_v^T x_v) for 7-point stencils S_v
+// ([7][N]: centre, W, E, S, N, below, above; entries pointing outside the
+// grid are ignored) and vectors x_v, one (vector, cell) per thread.
+__global__ void k_stencil_apply(int nz, int ny, int nx, const double* __restrict__ S_all,
+                                const double* __restrict__ x_all, double alpha, double beta, int trans,
+                                double* __restrict__ y_all) {
+  const int64_t N = (int64_t)nz * ny * nx;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const double* S = S_all + (int64_t)blockIdx.y * 7 * N;
+  const double* x = x_all + (int64_t)blockIdx.y * N;
+  double* y = y_all + (int64_t)blockIdx.y * N;
+  const int i = (int)(p % nx), j = (int)((p / nx) % ny), k = (int)(p / ((int64_t)nx * ny));
+  const int64_t off[7] = {0, -1, 1, -(int64_t)nx, (int64_t)nx, -(int64_t)nx * ny, (int64_t)nx * ny};
+  const bool ok[7] = {true, i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+  double acc = 0.0;
+  if (!trans) {
+#pragma unroll
+    for (int d = 0; d < 7; ++d)
+      if (ok[d]) acc += S[d * N + p] * x[p + off[d]];
+  } else {
+    // (S^T x)_p = sum over the rows q = p - off[d] whose entry d points at p
+    const bool okt[7] = {true, i < nx - 1, i > 0, j < ny - 1, j > 0, k < nz - 1, k > 0};
+#pragma unroll
+    for (int d = 0; d < 7; ++d)
+      if (okt[d]) acc += S[d * N + p - off[d]] * x[p - off[d]];
+  }
+  y[p] = (beta != 0.0 ? beta * y[p] : 0.0) + alpha * acc;
+}
+
 }  // namespace
+
+int stencil_apply(int nz, int ny, int nx, int n_vec, const double* S, const double* x, double alpha, double beta,
+                  int trans, double* y, cudaStream_t st) {
+  const int64_t N = (int64_t)nz * ny * nx;
+  dim3 g((unsigned)((N + 255) / 256), n_vec);
+  k_stencil_apply<<<g, 256, 0, st>>>(nz, ny, nx, S, x, alpha, beta, trans, y);
+  note_launch();
+  ORBIT_CUDA_TRY(cudaGetLastError());
+  return ORBIT_OK;
+}
 
 int assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T, double* rowsum,
                        cudaStream_t st) {

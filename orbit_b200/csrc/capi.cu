@@ -57,6 +57,8 @@ int fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec
                        double dt, int limited, double* d, cudaStream_t st);
 int fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
                         double* stencil, double* scratch, cudaStream_t st);
+int stencil_apply(int nz, int ny, int nx, int n_vec, const double* S, const double* x, double alpha, double beta,
+                  int trans, double* y, cudaStream_t st);
 
 namespace {
 
@@ -384,6 +386,15 @@ int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, in
   int rc = fct_linear_operator(nz, ny, nx, met, n_vec, c_base, dt, stencil, scratch, st);
   cudaFreeAsync(scratch, st);
   return rc;
+}
+
+int orbit_stencil_apply(int nz, int ny, int nx, int n_vec, const double* stencils, const double* x, double alpha,
+                        double beta, int trans, double* y, orbit_stream_t stream) {
+  if (!stencils || !x || !y || n_vec < 1 || nz < 1 || ny < 1 || nx < 1) {
+    set_last_error("orbit_stencil_apply: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  return stencil_apply(nz, ny, nx, n_vec, stencils, x, alpha, beta, trans, y, (cudaStream_t)stream);
 }
 
 int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,

@@ -98,6 +98,20 @@ def fct_linear_operator(met: MetDevice, c_base: torch.Tensor, dt: float = DTAU) 
     return out[0] if c_base.dim() == 1 else out
 
 
+def stencil_apply(nz: int, ny: int, nx: int, stencils: torch.Tensor, x: torch.Tensor, alpha: float = 1.0,
+                  trans: bool = False, out: Optional[torch.Tensor] = None, beta: float = 0.0) -> torch.Tensor:
+    """out = beta out + alpha S x (or S^T x) for [.., 7, N] stencils and [.., N] vectors."""
+    N = nz * ny * nx
+    S2 = stencils.reshape(-1, 7, N).contiguous()
+    x2 = x.reshape(-1, N).contiguous()
+    if S2.shape[0] != x2.shape[0]:
+        raise ValueError("one stencil per vector")
+    y = out if out is not None else torch.empty_like(x2)
+    _lib.check(_lib.lib().orbit_stencil_apply(nz, ny, nx, x2.shape[0], _lib.ptr(S2), _lib.ptr(x2), float(alpha),
+                                              float(beta), int(trans), _lib.ptr(y), _stream()))
+    return y.reshape(x.shape)
+
+
 def mass_balance(mets: Sequence[MetDevice], stencils: Sequence[torch.Tensor]) -> dict:
     """K7 row sums on the device, then the same order statistics the reference
     reports (operator.py:598-652): median, p90, p99, max of the interior rows
