@@ -97,11 +97,12 @@ int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_e
                              int subtree_div, orbit_symbolic_t* out);
 /* Replaces umfpack_free_symbolic (orbit/core/solve.py:291-296). */
 int orbit_symbolic_destroy(orbit_symbolic_t sym);
-/* info[0..12] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor
+/* info[0..14] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor
  * elements per instance, front elements per instance, max front, factor
  * flops, solve items per bin, update-vector length, leaf_cells, max n/m,
  * largest front inside a subtree solve task, floats of tensor-core operand
- * packs per fp32 instance. */
+ * packs per fp32 instance, supernodes factored whole by one CTA each
+ * (ORBIT_B200_FUSED_MAX_N, default 64, 0 = none). */
 int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info);
 /* perm[new] = cell (host array of N int32). */
 int orbit_symbolic_perm(orbit_symbolic_t sym, int32_t* perm_host);

@@ -227,6 +227,7 @@ int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_e
   opt.chunk_elems = std::max(256, chunk_elems > 0 ? chunk_elems : env_int("ORBIT_B200_CHUNK", kChunkElems));
   opt.tc_min_n = std::max(1, tc_min_n > 0 ? tc_min_n : env_int("ORBIT_B200_TC_MIN_N", opt.tc_min_n));
   opt.subtree_div = subtree_div >= 0 ? subtree_div : std::max(0, env_int("ORBIT_B200_SUBTREE_DIV", 0));
+  opt.fuse_max_n = std::max(0, env_int("ORBIT_B200_FUSED_MAX_N", kFrontMaxN));
   orbit_symbolic_s* h = new (std::nothrow) orbit_symbolic_s();
   if (!h) return ORBIT_ERR_NOMEM;
   std::string err = build_symbolic(nz, ny, nx, opt, h->S);
@@ -256,10 +257,10 @@ int orbit_symbolic_info(orbit_symbolic_t sym, int64_t* info, int n_info) {
     return ORBIT_ERR_ARG;
   }
   const Symbolic& S = sym->S;
-  int64_t v[14] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
+  int64_t v[15] = {S.N, S.nsuper, S.nlevels, S.fac_nnz, S.fac_size, S.front_buf_size, S.max_front,
                    (int64_t)S.factor_flops, S.sched[1].items_per_bin, S.w_size, S.leaf_cells, S.max_nm,
-                   S.max_sub_front, S.tc_pack_size};
-  for (int i = 0; i < n_info && i < 14; ++i) info[i] = v[i];
+                   S.max_sub_front, S.tc_pack_size, S.n_fused};
+  for (int i = 0; i < n_info && i < 15; ++i) info[i] = v[i];
   return ORBIT_OK;
 }
 

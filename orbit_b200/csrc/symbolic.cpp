@@ -287,8 +287,18 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
     S.fitems.push_back(a); S.fitems.push_back(b); S.fitems.push_back(c); S.fitems.push_back(d);
   };
   auto nitems = [&]() { return int64_t(S.fitems.size() / 4); };
+  S.fuse_max_n = std::max(0, std::min(kFrontMaxN, opt.fuse_max_n));
+  S.n_fused = 0;
   for (int l = S.nlevels - 1; l >= 0; --l) {
-    const auto& sups = S.level_sups[l];
+    const auto& all = S.level_sups[l];
+    // one-CTA fronts (FRONT) and the supernodes that take the blocked launches
+    std::vector<int32_t> fused, sups;
+    for (int s : all) {
+      const bool one = S.m[s] > 0 && S.n[s] > 0 && S.n[s] <= S.fuse_max_n &&
+                       front_smem_elems(S.n[s], S.m[s]) <= kFrontMaxElems;
+      (one ? fused : sups).push_back(s);
+    }
+    S.n_fused += int64_t(fused.size());
     std::vector<int> small, big;  // tensor-core nodes: n >= tc_min_n and m > 0
     for (int s : sups) {
       if (S.m[s] == 0 || S.n[s] == 0) continue;
@@ -299,7 +309,7 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
       // gathered through the inverse maps, zeros elsewhere; then the stencil
       // entries are added (SCATTER)
       int64_t off = nitems();
-      for (int s : sups) {
+      for (int s : all) {
         const int w = S.n[s] + S.m[s];
         const int rows = std::max(1, std::min(32, 8192 / std::max(1, int(S.ldf[s]))));
         for (int r0 = 0; r0 < w; r0 += rows) push_item(s, r0, std::min(w, r0 + rows), 0);
@@ -308,6 +318,25 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
     }
     S.fsched.push_back({FactorLaunch::SCATTER, l, 0, S.ent_level_off[l],
                         S.ent_level_off[l + 1] - S.ent_level_off[l]});
+    {
+      // one-CTA fronts in three shared-memory size classes, so that a launch
+      // of small fronts is not held to the occupancy of the largest one
+      const int64_t cls[3] = {4096, 12288, kFrontMaxElems};
+      std::vector<char> done(fused.size(), 0);
+      for (int c = 0; c < 3; ++c) {
+        const int64_t off = nitems();
+        int64_t emax = 0;
+        for (size_t q = 0; q < fused.size(); ++q) {
+          const int s = fused[q];
+          const int64_t e = front_smem_elems(S.n[s], S.m[s]);
+          if (done[q] || e > cls[c]) continue;
+          done[q] = 1;
+          emax = std::max(emax, e);
+          push_item(s, 0, 0, 0);
+        }
+        if (nitems() > off) S.fsched.push_back({FactorLaunch::FRONT, l, int(emax), off, nitems() - off});
+      }
+    }
     int nmax = 0;
     for (int s : sups) nmax = std::max(nmax, S.n[s]);
     for (int p0 = 0; p0 < nmax; p0 += kNB) {

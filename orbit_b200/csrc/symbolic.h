@@ -26,14 +26,25 @@ constexpr int kPad = 4;        // leading-dimension padding (elements)
 constexpr int kSchurTile = 128;  // output tile edge of the Schur-complement GEMM
 constexpr int kTcK = 16;         // K extent of one packed tensor-core operand tile
 constexpr int kTcTileFloats = kSchurTile * kTcK;  // floats per packed plane
+constexpr int kFrontMaxN = 64;        // largest pivot count of a one-CTA front
+constexpr int kFrontMaxElems = 28672;  // its shared-memory budget in elements (224 KB of FP64)
+
+// Shared-memory elements of a one-CTA front (k_front): the pivot block's
+// inverses and their transpose (n x ldq each), both panels (n x ldl each)
+// and the pivot steps' exchange slots (2 x 4 x 64).
+inline int64_t front_smem_elems(int64_t n, int64_t m) {
+  const int64_t ldq = (n + 3) / 4 * 4 + 4, ldl = (m + 3) / 4 * 4;
+  return 2 * n * ldq + 2 * n * ldl + 512;
+}
 
 inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 // One kernel launch of the numeric factorization schedule.
 struct FactorLaunch {
-  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU, TC_PACK, ASSEMBLE, TC_GEMM } kind;
+  enum Kind : int { ZERO = 0, SCATTER, EXTEND, DIAG, PANEL, UPDATE, SCHUR, INV, TRIL, PRODL, TRIU, PRODU, TC_PACK, ASSEMBLE, TC_GEMM, FRONT } kind;
   int level;
-  int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV); SCHUR: leading items of CUDA-core nodes
+  int p0;          // pivot-block start (DIAG/PANEL/UPDATE/INV); SCHUR: leading items of CUDA-core nodes;
+                   // FRONT: shared-memory elements of the largest front in the launch
   int64_t item_off;  // offset into the item array (int4 units)
   int64_t items;     // number of items (per instance)
 };
@@ -102,6 +113,10 @@ struct Symbolic {
   int tc_min_n = 0;
   std::vector<int64_t> tc_pack_off;
   int64_t tc_pack_size = 0;  // floats per instance (max over levels)
+  // one-CTA fronts: supernodes with 0 < n <= fuse_max_n, m > 0 and
+  // front_smem_elems(n, m) <= kFrontMaxElems are factored whole by one CTA
+  int fuse_max_n = 0;
+  int64_t n_fused = 0;
 };
 
 // Tuning options of the analysis (the autotuner's search space).
@@ -110,6 +125,7 @@ struct SymbolicOptions {
   int chunk_elems = 8192; // solve row-chunk size of the medium schedule (factor entries)
   int tc_min_n = 48;      // smallest pivot count of a tensor-core supernode (fp32 factors)
   int subtree_div = 0;    // > 0: whole-subtree solve tasks below fac_nnz / subtree_div; 0: none
+  int fuse_max_n = kFrontMaxN;  // largest pivot count of a one-CTA front (0: none)
 };
 
 // Build the symbolic analysis.  Returns an empty string on success, an

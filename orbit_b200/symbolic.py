@@ -20,7 +20,7 @@ _INT64_ARRAYS = {"ginv_off", "uoff", "fac_off", "front_off", "level_front_size",
 
 INFO_KEYS = ("N", "nsuper", "nlevels", "factor_nnz", "factor_elems", "front_elems", "max_front",
              "factor_flops", "solve_items_per_bin", "update_len", "leaf_cells", "max_nm",
-             "max_sub_front", "tc_pack_floats")
+             "max_sub_front", "tc_pack_floats", "fused_fronts")
 
 
 class Symbolic:

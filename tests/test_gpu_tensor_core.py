@@ -48,15 +48,19 @@ def test_tensor_core_schur_matches_cuda_cores():
     for k in range(n):
         spc = synthetic.make_species(20 + k, nz, ny, nx)
         sinks += [torch.as_tensor(d, device="cuda") for d in spc.sink_diag(met)]
-    old = os.environ.get("ORBIT_B200_TC_MIN_N")
+    # no one-CTA fronts: every supernode with n >= 16 takes the tensor cores
+    saved = {k: os.environ.get(k) for k in ("ORBIT_B200_TC_MIN_N", "ORBIT_B200_FUSED_MAX_N")}
     os.environ["ORBIT_B200_TC_MIN_N"] = "16"
+    os.environ["ORBIT_B200_FUSED_MAX_N"] = "0"
     try:
         sym = Symbolic(nz, ny, nx, 32)
     finally:
-        if old is None:
-            del os.environ["ORBIT_B200_TC_MIN_N"]
-        else:
-            os.environ["ORBIT_B200_TC_MIN_N"] = old
+        for k, v in saved.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
+    assert sym.info["fused_fronts"] == 0
     x = torch.as_tensor(rng.standard_normal((n, sym.N)), device="cuda")
     ref = _chain(sym, T, sinks, 64, x, "1")
     y_tc = _chain(sym, T, sinks, 32, x, "1")
