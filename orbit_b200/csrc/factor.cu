@@ -616,16 +616,17 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
 // A supernode with n <= 64 pivots whose pivot-block inverses and panels fit
 // in shared memory is factored whole by one CTA, which does what the DIAG,
 // PANEL, UPDATE, INV, TRIL/TRIU, PRODL/PRODU and SCHUR launches do for the
-// larger ones: unpivoted LU of F11, the explicit inverses (stored as SQ),
-// L21 = F21 inv(U11) and U12 = inv(L11) F12 in place, then
-// Pb = -L21 inv(L11), Qr = -inv(U11) U12 and F22 -= L21 U12.  The deepest
+// larger ones: unpivoted LU of F11 with the explicit inverses (stored as SQ),
+// X = inv(U11) inv(L11) (= inv(F11)), Pb = -F21 X, Qr = -X F12 and
+// F22 += Pb F12 (the products the tensor-core pipeline forms).  The deepest
 // levels of the dissection are thousands of such fronts per instance, which
 // the multi-launch path runs at a few per cent of the GPU.  Shared memory
 // (ldq = round_up(n, 4) + 4, ldl = round_up(m, 4); front_smem_elems):
-//   Q  [n][ldq]  strict lower inv(L11), upper inv(U11)     (= SQ)
-//   Qt [n][ldq]  the LU of F11 until the inverses are formed, then Q^T
-//   Lt [n][ldl]  F21^T, then L21^T
-//   U  [n][ldl]  F12, then U12
+//   Q  [n][ldq]  strict lower inv(L11), upper inv(U11) (= SQ), then X
+//   Qt [n][ldq]  the staged F11 until the inverses are formed, then Q^T, then X^T
+//   Lt [n][ldl]  F21^T, then Pb^T
+//   U  [n][ldl]  F12
+//   ex [2][4][64] exchange slots of the pivot steps
 
 // 4 consecutive elements from 16-byte aligned shared memory.
 template <typename T>
@@ -657,26 +658,22 @@ __device__ __forceinline__ void sts4(T* p, T a, T b, T c, T d) {
   }
 }
 
-// One step j of a 4 x 4 block product: acc(i, q) += A(r + i, j) B(j, c + q),
-// A read as At[j * lda + r], B as Bm[j * ldb + c]; with MASK the triangular
-// operand of MODE (front_block) is zeroed outside its triangle.
-template <typename T, int MODE, bool MASK>
-__device__ __forceinline__ void fb_step(const T* At, int lda, const T* Bm, int ldb, int j, int r, int c,
+// One step k of a 4 x 4 block product: acc(i, q) += A(r + i, k) B(k, c + q)
+// with A read as At[k * lda + r] and B as Bm[k * ldb + c]; with MASK the
+// terms outside k >= r + i (A = inv(U11)) and k > c + q (B = inv(L11)) vanish.
+template <typename T, bool MASK>
+__device__ __forceinline__ void fb_step(const T* At, int lda, const T* Bm, int ldb, int k, int r, int c,
                                         T (&acc)[4][4]) {
   T a[4], b[4];
-  lds4(At + j * lda + r, a);
-  lds4(Bm + j * ldb + c, b);
+  lds4(At + k * lda + r, a);
+  lds4(Bm + k * ldb + c, b);
   if (MASK) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      if (MODE == 1 && !(j < r + i)) a[i] = T(0);
-      if (MODE == 2 && !(j >= r + i)) a[i] = T(0);
-    }
+    for (int i = 0; i < 4; ++i)
+      if (!(k >= r + i)) a[i] = T(0);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (MODE == 0 && !(j <= c + q)) b[q] = T(0);
-      if (MODE == 3 && !(j > c + q)) b[q] = T(0);
-    }
+    for (int q = 0; q < 4; ++q)
+      if (!(k > c + q)) b[q] = T(0);
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -684,48 +681,141 @@ __device__ __forceinline__ void fb_step(const T* At, int lda, const T* Bm, int l
     for (int q = 0; q < 4; ++q) acc[i][q] = fma(a[i], b[q], acc[i][q]);
 }
 
-// acc(i, q) = sum_j A(r + i, j) B(j, c + q) for this thread's 4 x 4 block at
-// (r, c) (multiples of 4), j < K.  MODE fixes which operand is triangular:
-//   0  B = inv(U11) (rows of Q), j <= c                    L21 = F21 inv(U11)
-//   1  A = inv(L11) (rows of Qt), j < r, plus B(r, c)      U12 = inv(L11) F12
-//   2  A = inv(U11) (rows of Qt), j >= r                   inv(U11) U12
-//   3  B = inv(L11) (rows of Q), j > c, plus A(r, c)       L21 inv(L11)
-//   4  dense                                               L21 U12
-// The mask only matters for the three j next to the block's diagonal, so the
-// loop runs unmasked elsewhere.
-template <typename T, int MODE>
+// Dense 4 x 4 block product over k < K (block at (r, c), multiples of 4).
+template <typename T>
 __device__ __forceinline__ void front_block(const T* At, int lda, const T* Bm, int ldb, int K, int r, int c,
                                             T (&acc)[4][4]) {
   zero_acc(acc);
-  if (MODE == 1) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (r + i < K) {
-        T v[4];
-        lds4(Bm + (r + i) * ldb + c, v);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[i][q] = v[q];
-      }
-  }
-  if (MODE == 3) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      if (c + q < K) {
-        T v[4];
-        lds4(At + (c + q) * lda + r, v);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) acc[i][q] = v[i];
-      }
-  }
-  // unmasked range [u0, u1) and masked range [m0, m1)
-  int u0 = 0, u1 = K, m0 = 0, m1 = 0;
-  if (MODE == 0) { u1 = min(K, c + 1); m0 = u1; m1 = min(K, c + 4); }
-  if (MODE == 1) { u1 = min(K, r); m0 = u1; m1 = min(K, r + 3); }
-  if (MODE == 2) { m0 = r; m1 = min(K, r + 3); u0 = m1; }
-  if (MODE == 3) { m0 = c + 1; m1 = min(K, c + 4); u0 = max(m1, m0); }
-  for (int j = m0; j < m1; ++j) fb_step<T, MODE, true>(At, lda, Bm, ldb, j, r, c, acc);
 #pragma unroll 4
-  for (int j = u0; j < u1; ++j) fb_step<T, MODE, false>(At, lda, Bm, ldb, j, r, c, acc);
+  for (int k = 0; k < K; ++k) fb_step<T, false>(At, lda, Bm, ldb, k, r, c, acc);
+}
+
+// X(r + i, c + q) = sum over k >= max(r + i, c + q) of inv(U11)(r + i, k)
+// inv(L11)(k, c + q): the unit diagonal of inv(L11) gives the k = c + q term
+// inv(U11)(r + i, c + q), the rest runs over k > c with both triangles masked
+// only next to the block's diagonals.  inv(U11)(r, k) = Q[r][k] = Qt[k][r]
+// (k >= r), inv(L11)(k, c) = Q[k][c] (k > c).
+template <typename T>
+__device__ __forceinline__ void front_x_block(const T* Q, const T* Qt, int ldq, int n, int r, int c,
+                                              T (&acc)[4][4]) {
+  zero_acc(acc);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (c + q < n) {
+      T v[4];
+      lds4(Qt + (c + q) * ldq + r, v);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[i][q] = (c + q >= r + i) ? v[i] : T(0);
+    }
+  const int k0 = max(r, c + 1), k1 = min(n, max(r + 3, c + 4));
+  for (int k = k0; k < k1; ++k) fb_step<T, true>(Qt, ldq, Q, ldq, k, r, c, acc);
+#pragma unroll 4
+  for (int k = max(k0, k1); k < n; ++k) fb_step<T, false>(Qt, ldq, Q, ldq, k, r, c, acc);
+}
+
+// Unpivoted LU of the staged F11 (Dm) with inv(L11) and inv(U11)^T formed in
+// the same pivot steps, one barrier per step; the result goes to Q (strict
+// lower inv(L11), upper inv(U11)) and Qt = Q^T.  Thread (ty, tx) holds rows
+// ty + 16a and columns tx + 16b (a, b < G, n <= 16 G) of A (F11, becoming
+// the LU), X (inv(L11)) and Z (inv(U11)^T, by forward substitution on U^T:
+// row k of U is final at step k).  At step k the holders of row k publish
+// its A, X and Z values, those of column k its A values; after the barrier
+// every thread applies, for its rows i > k,
+//   A(i, j) -= l_i A(k, j)  (j > k; l_i = A(i, k) / A(k, k) is stored at j = k)
+//   X(i, j) -= l_i X(k, j)
+//   Z(i, j) -= A(k, i) z_j  (z_j = Z(k, j) / A(k, k), stored in row k).
+// Row and column groups of 16 that a step cannot touch are skipped; the
+// exchange slots alternate between two sets so that one barrier per step
+// orders every write after the previous step's reads.
+template <typename T, int G>
+__device__ __forceinline__ void front_lu(const T* Dm, T* Q, T* Qt, T* ex, int n, int ldq, int* status) {
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T A[G][G], X[G][G], Z[G][G];
+#pragma unroll
+  for (int a = 0; a < G; ++a)
+#pragma unroll
+    for (int b = 0; b < G; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      A[a][b] = (i < n && j < n) ? Dm[i * ldq + j] : T(0);
+      X[a][b] = Z[a][b] = (i == j) ? T(1) : T(0);
+    }
+  for (int k = 0; k < n; ++k) {
+    T* pr = ex + (k & 1) * 256;
+    T* lc = pr + 64;
+    T* xr = lc + 64;
+    T* zr = xr + 64;
+    const int kr = k & 15, kg = k >> 4;
+    if (ty == kr) {
+#pragma unroll
+      for (int a = 0; a < G; ++a)
+        if (a == kg) {
+#pragma unroll
+          for (int b = 0; b < G; ++b) {
+            const int j = tx + 16 * b;
+            pr[j] = A[a][b];
+            xr[j] = X[a][b];
+            zr[j] = Z[a][b];
+          }
+        }
+    }
+    if (tx == kr) {
+#pragma unroll
+      for (int b = 0; b < G; ++b)
+        if (b == kg) {
+#pragma unroll
+          for (int a = 0; a < G; ++a) lc[ty + 16 * a] = A[a][b];
+        }
+    }
+    __syncthreads();
+    const T piv = pr[k];
+    if (tid == 0 && (!(piv == piv) || piv == T(0) || isinf((double)piv))) raise_status(status, ORBIT_ERR_PIVOT);
+    const T rp = T(1) / piv;
+    T pj[G], xj[G], zj[G];
+#pragma unroll
+    for (int b = 0; b < G; ++b) {
+      const int j = tx + 16 * b;
+      pj[b] = j > k ? pr[j] : T(0);
+      xj[b] = xr[j];
+      zj[b] = zr[j] * rp;
+    }
+#pragma unroll
+    for (int a = 0; a < G; ++a) {
+      if (16 * a + 15 < k) continue;  // every row of the group is above the pivot
+      const int i = ty + 16 * a;
+      const bool below = i > k;
+      const T l = below ? lc[i] * rp : T(0);
+      const T u = below ? pr[i] : T(0);
+#pragma unroll
+      for (int b = 0; b < G; ++b) {
+        if (16 * b + 15 > k) A[a][b] -= l * pj[b];  // columns j > k exist in the group
+        if (16 * b <= k) {                          // X(k, j), Z(k, j) vanish for j > k
+          X[a][b] -= l * xj[b];
+          Z[a][b] = (i == k) ? zj[b] : Z[a][b] - u * zj[b];
+        }
+      }
+      if (below && tx == kr) {
+#pragma unroll
+        for (int b = 0; b < G; ++b)
+          if (b == kg) A[a][b] = l;
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < G; ++a)
+#pragma unroll
+    for (int b = 0; b < G; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      if (i < n && j < n) {
+        if (i > j) {
+          Q[i * ldq + j] = X[a][b];
+          Qt[j * ldq + i] = X[a][b];
+        }
+        if (i >= j) {
+          Q[j * ldq + i] = Z[a][b];
+          Qt[i * ldq + j] = Z[a][b];
+        }
+      }
+    }
 }
 
 template <typename T>
@@ -739,18 +829,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_front(FactorDev
   T* Qt = Q + n * ldq;
   T* Lt = Qt + n * ldq;
   T* U = Lt + n * ldl;
-  T* Dm = Qt;
+  T* ex = U + n * ldl;
   T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
   T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
   T* Pb = SQ + (int64_t)n * ldn;
   T* Qr = SQ + (int64_t)(n + m) * ldn;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  // 1. F11, F12 and F21^T into shared memory by asynchronous element copies
-  // (rows by warps, columns by lanes), all in flight before the wait
+  // 1. F11 (into Qt's space), F12 and F21^T into shared memory by
+  // asynchronous element copies (rows by warps, columns by lanes), all in
+  // flight before the wait
   for (int r = warp; r < n; r += kThreads / 32) {
     const T* row = F + (int64_t)r * ldf;
-    for (int c = lane; c < n + m; c += 32) cp_async_elem(c < n ? Dm + r * ldq + c : U + r * ldl + (c - n), row + c);
+    for (int c = lane; c < n + m; c += 32) cp_async_elem(c < n ? Qt + r * ldq + c : U + r * ldl + (c - n), row + c);
   }
   for (int r = warp; r < m; r += kThreads / 32) {
     const T* row = F + (int64_t)(n + r) * ldf;
@@ -759,152 +850,51 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_front(FactorDev
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
 
-  // 2. unpivoted LU of F11 with inv(L11) and inv(U11)^T formed alongside,
-  // one barrier per pivot step.  Thread (ty, tx) holds rows ty + 16a and
-  // columns tx + 16b (a, b < 4) of A (F11, becoming the LU), X (inv(L11))
-  // and Z (inv(U11)^T, by forward substitution on U^T: row k of U is final
-  // at step k).  At step k the holders of row k publish its A, X and Z
-  // values, those of column k its A values; after the barrier every thread
-  // applies, for its rows i > k,
-  //   A(i, j) -= l_i A(k, j)  (j > k; l_i = A(i, k) / A(k, k) is stored at j = k)
-  //   X(i, j) -= l_i X(k, j)
-  //   Z(i, j) -= A(k, i) z_j  (z_j = Z(k, j) / A(k, k), stored in row k)
-  // The exchange slots alternate between two sets, so one barrier per step
-  // orders every write after the previous step's reads.
-  {
-    T* ex = U + n * ldl;  // 2 x (pivot row, column k, row k of X, row k of Z), 64 each
-    const int tx = tid & 15, ty = tid >> 4;
-    T A[4][4], X[4][4], Z[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int i = ty + 16 * a, j = tx + 16 * b;
-        A[a][b] = (i < n && j < n) ? Dm[i * ldq + j] : T(0);
-        X[a][b] = Z[a][b] = (i == j) ? T(1) : T(0);
-      }
-    for (int k = 0; k < n; ++k) {
-      T* pr = ex + (k & 1) * 256;
-      T* lc = pr + 64;
-      T* xr = lc + 64;
-      T* zr = xr + 64;
-      const int kr = k & 15, kg = k >> 4;
-      if (ty == kr) {
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-          if (a == kg) {
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-              const int j = tx + 16 * b;
-              pr[j] = A[a][b];
-              xr[j] = X[a][b];
-              zr[j] = Z[a][b];
-            }
-          }
-      }
-      if (tx == kr) {
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (b == kg) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) lc[ty + 16 * a] = A[a][b];
-          }
-      }
-      __syncthreads();
-      const T piv = pr[k];
-      if (tid == 0 && (!(piv == piv) || piv == T(0) || isinf((double)piv))) raise_status(status, ORBIT_ERR_PIVOT);
-      const T rp = T(1) / piv;
-      T pj[4], xj[4], zj[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int j = tx + 16 * b;
-        pj[b] = pr[j];
-        xj[b] = xr[j];
-        zj[b] = zr[j] * rp;
-      }
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = ty + 16 * a;
-        if (i > k) {
-          const T l = lc[i] * rp, u = pr[i];
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const int j = tx + 16 * b;
-            if (j > k) A[a][b] -= l * pj[b];
-            else if (j == k) A[a][b] = l;
-            X[a][b] -= l * xj[b];
-            Z[a][b] -= u * zj[b];
-          }
-        } else if (i == k) {
-#pragma unroll
-          for (int b = 0; b < 4; ++b) Z[a][b] = zj[b];
-        }
-      }
-    }
-    // 3. Q = strict_lower(inv(L11)) + upper(inv(U11)) and its transpose
-    // (over the staged F11, no longer read)
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int i = ty + 16 * a, j = tx + 16 * b;
-        if (i < n && j < n) {
-          if (i > j) {
-            Q[i * ldq + j] = X[a][b];
-            Qt[j * ldq + i] = X[a][b];
-          }
-          if (i >= j) {
-            Q[j * ldq + i] = Z[a][b];
-            Qt[i * ldq + j] = Z[a][b];
-          }
-        }
-      }
-  }
+  // 2. LU and both triangular inverses into Q / Qt, register blocks sized to n
+  if (n <= 16) front_lu<T, 1>(Qt, Q, Qt, ex, n, ldq, status);
+  else if (n <= 32) front_lu<T, 2>(Qt, Q, Qt, ex, n, ldq, status);
+  else if (n <= 48) front_lu<T, 3>(Qt, Q, Qt, ex, n, ldq, status);
+  else front_lu<T, 4>(Qt, Q, Qt, ex, n, ldq, status);
   __syncthreads();
 
-  // 4. SQ to the factor storage
+  // 3. SQ to the factor storage; X = inv(U11) inv(L11) into registers, then
+  // over Q (and X^T over Qt) once every thread has read them
   for (int r = warp; r < n; r += kThreads / 32)
     for (int c = lane; c < n; c += 32) SQ[(int64_t)r * ldn + c] = Q[r * ldq + c];
-
-  // thread layouts: n-wide operands take as few lanes as cover n / 4
-  const int wn = n <= 16 ? 4 : n <= 32 ? 8 : 16;  // threads across n
-  const int wo = kThreads / wn;                   // threads across m
+  const int wn = (n + 3) >> 2;        // threads across n (4 columns each)
+  const int wo = kThreads / wn;       // threads across m
   const int an = tid % wn, ao = tid / wn;
-
-  // 5. L21 = F21 inv(U11) in place (blocks of L21 rows), then
-  //    U12 = inv(L11) F12 in place (blocks of U12 columns); a block reads only
-  //    its own rows (columns), so one barrier before its stores suffices
-  for (int rb = 0; rb < m; rb += 4 * wo) {
-    const int r = rb + 4 * ao, c = 4 * an;
-    const bool act = r < m && c < n;
-    T acc[4][4];
-    if (act) front_block<T, 0>(Lt, ldl, Q, ldq, n, r, c, acc);
-    __syncthreads();
-    if (act)
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (c + q < n) sts4(Lt + (int64_t)(c + q) * ldl + r, acc[0][q], acc[1][q], acc[2][q], acc[3][q]);
-  }
-  for (int cb = 0; cb < m; cb += 4 * wo) {
-    const int r = 4 * an, c = cb + 4 * ao;
-    const bool act = r < n && c < m;
-    T acc[4][4];
-    if (act) front_block<T, 1>(Qt, ldq, U, ldl, n, r, c, acc);
+  {
+    const bool act = tid < wn * wn;
+    const int r = 4 * (tid / wn), c = 4 * (tid % wn);
+    T x[4][4];
+    if (act) front_x_block<T>(Q, Qt, ldq, n, r, c, x);
     __syncthreads();
     if (act)
 #pragma unroll
       for (int i = 0; i < 4; ++i)
-        if (r + i < n) sts4(U + (int64_t)(r + i) * ldl + c, acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (r + i < n && c + q < n) {
+            Q[(r + i) * ldq + c + q] = x[i][q];
+            Qt[(c + q) * ldq + r + i] = x[i][q];
+          }
   }
   __syncthreads();
 
-  // 6. Pb = -L21 inv(L11) and Qr = -inv(U11) U12 into the factor storage
-  // (padding columns untouched), then F22 -= L21 U12 in the front
+  // 4. Pb = -F21 X to the factor storage (padding columns untouched) and,
+  // in place of F21^T, as Pb^T for the Schur complement; a block of Pb rows
+  // reads only its own columns of Lt, so one barrier before its stores suffices
   for (int rb = 0; rb < m; rb += 4 * wo) {
     const int r = rb + 4 * ao, c = 4 * an;
-    if (r < m && c < n) {
-      T acc[4][4];
-      front_block<T, 3>(Lt, ldl, Q, ldq, n, r, c, acc);
+    const bool act = ao < wo && r < m;
+    T acc[4][4];
+    if (act) front_block<T>(Lt, ldl, Q, ldq, n, r, c, acc);
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (c + q < n) sts4(Lt + (c + q) * ldl + r, -acc[0][q], -acc[1][q], -acc[2][q], -acc[3][q]);
 #pragma unroll
       for (int i = 0; i < 4; ++i)
         if (r + i < m) {
@@ -919,11 +909,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_front(FactorDev
         }
     }
   }
+  __syncthreads();
+
+  // 5. Qr = -X F12 to the factor storage, then F22 += Pb F12 in the front
   for (int cb = 0; cb < m; cb += 4 * wo) {
     const int r = 4 * an, c = cb + 4 * ao;
-    if (r < n && c < m) {
+    if (ao < wo && c < m) {
       T acc[4][4];
-      front_block<T, 2>(Qt, ldq, U, ldl, n, r, c, acc);
+      front_block<T>(Qt, ldq, U, ldl, n, r, c, acc);
 #pragma unroll
       for (int i = 0; i < 4; ++i)
         if (r + i < n) {
@@ -959,12 +952,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_front(FactorDev
       const int r = (t / mt) * 64 + 4 * ty, c = (t % mt) * 64 + 4 * tx;
       if (r < m && c < m) {
         T acc[4][4];
-        front_block<T, 4>(Lt, ldl, U, ldl, n, r, c, acc);
+        front_block<T>(Lt, ldl, U, ldl, n, r, c, acc);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (r + i < m && c + q < m) F22[(int64_t)(r + i) * ldf + c + q] = cv[i][q] - acc[i][q];
+            if (r + i < m && c + q < m) F22[(int64_t)(r + i) * ldf + c + q] = cv[i][q] + acc[i][q];
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
