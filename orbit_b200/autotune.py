@@ -28,7 +28,7 @@ import numpy as np
 
 DEFAULTS = {"leaf_cells": 64, "chunk_elems": 8192, "tc_min_n": 48, "subtree_div": 0}
 SPACE = {
-    "leaf_cells": [48, 64, 96],
+    "leaf_cells": [48, 64, 80, 96],
     "chunk_elems": [4096, 8192, 16384],
     "tc_min_n": [32, 48, 96],
     "subtree_div": [0, 1024],
