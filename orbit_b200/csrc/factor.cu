@@ -197,33 +197,45 @@ __global__ void __launch_bounds__(256) k_assemble(FactorDev D, T* fr, const T* f
     const T* s0 = u0 >= 0 ? Sc[0] + (int64_t)u0 * ldc[0] : nullptr;
     const T* s1 = u1 >= 0 ? Sc[1] + (int64_t)u1 * ldc[1] : nullptr;
     T* row = F + (int64_t)i * ldf;
-    for (int j0 = 4 * lane; j0 < ldf; j0 += 128) {
-      T v[4] = {T(0), T(0), T(0), T(0)};
-      if (j0 < wp) {
-        if (s0) {
-          const int4 c = sinv4[j0 >> 2];
-          if (c.x >= 0) v[0] += s0[c.x];
-          if (c.y >= 0) v[1] += s0[c.y];
-          if (c.z >= 0) v[2] += s0[c.z];
-          if (c.w >= 0) v[3] += s0[c.w];
-        }
-        if (s1) {
-          const int4 c = sinv4[(wp + j0) >> 2];
-          if (c.x >= 0) v[0] += s1[c.x];
-          if (c.y >= 0) v[1] += s1[c.y];
-          if (c.z >= 0) v[2] += s1[c.z];
-          if (c.w >= 0) v[3] += s1[c.w];
+    // two 128-column chunks per iteration: all gathers in flight before the stores
+    for (int jb = 4 * lane; jb < ldf; jb += 256) {
+      T v[2][4];
+#pragma unroll
+      for (int g = 0; g < 2; ++g) {
+        const int j0 = jb + 128 * g;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) v[g][h] = T(0);
+        if (j0 < wp) {
+          if (s0) {
+            const int4 c = sinv4[j0 >> 2];
+            if (c.x >= 0) v[g][0] += s0[c.x];
+            if (c.y >= 0) v[g][1] += s0[c.y];
+            if (c.z >= 0) v[g][2] += s0[c.z];
+            if (c.w >= 0) v[g][3] += s0[c.w];
+          }
+          if (s1) {
+            const int4 c = sinv4[(wp + j0) >> 2];
+            if (c.x >= 0) v[g][0] += s1[c.x];
+            if (c.y >= 0) v[g][1] += s1[c.y];
+            if (c.z >= 0) v[g][2] += s1[c.z];
+            if (c.w >= 0) v[g][3] += s1[c.w];
+          }
         }
       }
 #pragma unroll
-      for (int h = 0; h < 4; h += VW) {
-        V x;
-        if constexpr (VW == 4) {
-          x.x = v[0]; x.y = v[1]; x.z = v[2]; x.w = v[3];
-        } else {
-          x.x = v[h]; x.y = v[h + 1];
+      for (int g = 0; g < 2; ++g) {
+        const int j0 = jb + 128 * g;
+        if (j0 >= ldf) break;
+#pragma unroll
+        for (int h = 0; h < 4; h += VW) {
+          V x;
+          if constexpr (VW == 4) {
+            x.x = v[g][0]; x.y = v[g][1]; x.z = v[g][2]; x.w = v[g][3];
+          } else {
+            x.x = v[g][h]; x.y = v[g][h + 1];
+          }
+          *reinterpret_cast<V*>(row + j0 + h) = x;
         }
-        *reinterpret_cast<V*>(row + j0 + h) = x;
       }
     }
   }
@@ -1012,13 +1024,14 @@ __device__ __forceinline__ void store_split4(float* tile, int off, float a, floa
   *reinterpret_cast<float4*>(tile + tc::kTileFloats + off) = lo;
 }
 
-// One 128 x 16 operand tile: op 0 F21 and op 2 inv(U11) (A side: rows x K,
-// read along rows), op 1 F12^T and op 3 inv(L11)^T with its unit diagonal
-// (B side: columns x K, read down columns).
+// A run of kTcPackRun 128 x 16 operand tiles of one row tile: op 0 F21 and
+// op 2 inv(U11) (A side: rows x K, read along rows), op 1 F12^T and op 3
+// inv(L11)^T with its unit diagonal (B side: columns x K, read down columns).
+// Every load of the run is issued before the first store.
 __global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* fronts, const float* factors,
                                                  float* pack, int64_t i0, int inst_base) {
   const int4 it = D.items[i0 + blockIdx.x];
-  const int s = it.x, op = it.y, t = it.z, kb = it.w;
+  const int s = it.x, op = it.y, t = it.z, kb0 = it.w;
   const int n = D.n[s], m = D.m[s], ldf = D.ldf[s], ldn = D.ldn[s];
   const int mt = (m + 127) / 128, nt = (n + 127) / 128, kt = (n + tc::kCols - 1) / tc::kCols;
   const float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
@@ -1026,30 +1039,46 @@ __global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* front
   const int region = op;
   const int rows = op <= 1 ? m : n;
   const bool bside = op == 1 || op == 3;
-  float* dst = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s] + tc_tile(region, t, kb, mt, nt, kt);
-  for (int q = threadIdx.x; q < tc::kRows * (tc::kCols / 4); q += blockDim.x) {
-    // A side: 4 consecutive threads read one 64-byte row segment; B side:
-    // consecutive threads read consecutive columns of one source row.
-    const int r = bside ? q & 127 : q >> 2;
-    const int c = bside ? q >> 7 : q & 3;
-    const int row = t * tc::kRows + r;
-    const int k = kb * tc::kCols + c * 4;
-    float v[4];
+  float* dst0 = pack + (int64_t)blockIdx.y * D.tc_pack_stride + D.tc_pack_off[s];
+  constexpr int kPer = tc::kRows * (tc::kCols / 4) / 256;  // 16-byte chunks per thread and tile
+  float v[kTcPackRun][kPer][4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int kk = k + u;
-      float x = 0.f;
-      if (row < rows && kk < n) {
-        switch (op) {
-          case 0: x = F[(int64_t)(n + row) * ldf + kk]; break;
-          case 1: x = F[(int64_t)kk * ldf + n + row]; break;
-          case 2: x = kk >= row ? SQ[(int64_t)row * ldn + kk] : 0.f; break;
-          default: x = row < kk ? SQ[(int64_t)kk * ldn + row] : (row == kk ? 1.f : 0.f); break;
+  for (int h = 0; h < kTcPackRun; ++h)
+#pragma unroll
+    for (int p = 0; p < kPer; ++p) {
+      // A side: 4 consecutive threads read one 64-byte row segment; B side:
+      // consecutive threads read consecutive columns of one source row.
+      const int q = threadIdx.x + 256 * p;
+      const int r = bside ? q & 127 : q >> 2;
+      const int c = bside ? q >> 7 : q & 3;
+      const int row = t * tc::kRows + r;
+      const int k = (kb0 + h) * tc::kCols + c * 4;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int kk = k + u;
+        float x = 0.f;
+        if (row < rows && kk < n) {
+          switch (op) {
+            case 0: x = F[(int64_t)(n + row) * ldf + kk]; break;
+            case 1: x = F[(int64_t)kk * ldf + n + row]; break;
+            case 2: x = kk >= row ? SQ[(int64_t)row * ldn + kk] : 0.f; break;
+            default: x = row < kk ? SQ[(int64_t)kk * ldn + row] : (row == kk ? 1.f : 0.f); break;
+          }
         }
+        v[h][p][u] = x;
       }
-      v[u] = x;
     }
-    store_split4(dst, tc::swz(r, c * 4), v[0], v[1], v[2], v[3]);
+#pragma unroll
+  for (int h = 0; h < kTcPackRun; ++h) {
+    if (kb0 + h >= kt) break;
+    float* dst = dst0 + tc_tile(region, t, kb0 + h, mt, nt, kt);
+#pragma unroll
+    for (int p = 0; p < kPer; ++p) {
+      const int q = threadIdx.x + 256 * p;
+      const int r = bside ? q & 127 : q >> 2;
+      const int c = bside ? q >> 7 : q & 3;
+      store_split4(dst, tc::swz(r, c * 4), v[h][p][0], v[h][p][1], v[h][p][2], v[h][p][3]);
+    }
   }
 }
 

@@ -311,7 +311,7 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
       int64_t off = nitems();
       for (int s : all) {
         const int w = S.n[s] + S.m[s];
-        const int rows = std::max(1, std::min(32, 8192 / std::max(1, int(S.ldf[s]))));
+        const int rows = 32;
         for (int r0 = 0; r0 < w; r0 += rows) push_item(s, r0, std::min(w, r0 + rows), 0);
       }
       S.fsched.push_back({FactorLaunch::ASSEMBLE, l, 0, off, nitems() - off});
@@ -448,7 +448,7 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
           for (int op : ops) {
             const int tiles = (op == 0 || op == 1 || op == 6) ? mt : nt;
             for (int t = 0; t < tiles; ++t)
-              for (int k = 0; k < kt; ++k) push_item(s, op, t, k);
+              for (int k = 0; k < kt; k += kTcPackRun) push_item(s, op, t, k);
           }
         }
         S.fsched.push_back({FactorLaunch::TC_PACK, l, 0, off, nitems() - off});

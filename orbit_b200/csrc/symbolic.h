@@ -26,6 +26,7 @@ constexpr int kPad = 4;        // leading-dimension padding (elements)
 constexpr int kSchurTile = 128;  // output tile edge of the Schur-complement GEMM
 constexpr int kTcK = 16;         // K extent of one packed tensor-core operand tile
 constexpr int kTcTileFloats = kSchurTile * kTcK;  // floats per packed plane
+constexpr int kTcPackRun = 4;        // k-blocks of one operand row tile packed by one CTA
 constexpr int kFrontMaxN = 64;        // largest pivot count of a one-CTA front
 constexpr int kFrontMaxElems = 28672;  // its shared-memory budget in elements (224 KB of FP64)
 
