@@ -242,87 +242,6 @@ __global__ void __launch_bounds__(256) k_assemble(FactorDev D, T* fr, const T* f
 }
 
 template <typename T>
-__global__ void k_diag(FactorDev D, T* fronts, T* factors, int64_t i0, int p0, int inst_base,
-                       int* status) {
-  extern __shared__ unsigned char smem_raw[];
-  T* Dm = reinterpret_cast<T*>(smem_raw);
-  T* Li = Dm + 64 * kLdS;
-  T* Ui = Li + 64 * kLdS;
-  const int s = D.items[i0 + blockIdx.x].x;
-  const int n = D.n[s];
-  const int nb = min(64, n - p0);
-  const int ldf = D.ldf[s], ldn = D.ldn[s];
-  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
-  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s];
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  // element loops use a fixed 64-wide index space (no divisions by nb)
-  for (int e = tid; e < 64 * 64; e += kThreads) {
-    const int r = e >> 6, c = e & 63;
-    if (r < nb && c < nb) Dm[r * kLdS + c] = F[(int64_t)(p0 + r) * ldf + p0 + c];
-  }
-  __syncthreads();
-  for (int k = 0; k < nb; ++k) {
-    T piv = Dm[k * kLdS + k];
-    if (tid == 0 && (!(piv == piv) || piv == T(0) || isinf((double)piv)))
-      raise_status(status, ORBIT_ERR_PIVOT);
-    for (int i = k + 1 + tid; i < nb; i += kThreads) Dm[i * kLdS + k] /= piv;
-    __syncthreads();
-    for (int i = k + 1 + ty; i < nb; i += 16) {
-      const T l = Dm[i * kLdS + k];
-      for (int j = k + 1 + tx; j < nb; j += 16) Dm[i * kLdS + j] -= l * Dm[k * kLdS + j];
-    }
-    __syncthreads();
-  }
-  // explicit inverses, one column per thread; four partial sums shorten the
-  // dependent chain of each entry
-  if (tid < 64) {
-    const int j = tid;
-    if (j < nb) {
-      for (int i = 0; i < j; ++i) Li[i * kLdS + j] = T(0);
-      Li[j * kLdS + j] = T(1);
-      for (int i = j + 1; i < nb; ++i) {
-        T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-        int k = j;
-        for (; k + 3 < i; k += 4) {
-          a0 -= Dm[i * kLdS + k] * Li[k * kLdS + j];
-          a1 -= Dm[i * kLdS + k + 1] * Li[(k + 1) * kLdS + j];
-          a2 -= Dm[i * kLdS + k + 2] * Li[(k + 2) * kLdS + j];
-          a3 -= Dm[i * kLdS + k + 3] * Li[(k + 3) * kLdS + j];
-        }
-        for (; k < i; ++k) a0 -= Dm[i * kLdS + k] * Li[k * kLdS + j];
-        Li[i * kLdS + j] = (a0 + a1) + (a2 + a3);
-      }
-    }
-  } else if (tid < 128) {
-    const int j = tid - 64;
-    if (j < nb) {
-      for (int i = j + 1; i < nb; ++i) Ui[i * kLdS + j] = T(0);
-      Ui[j * kLdS + j] = T(1) / Dm[j * kLdS + j];
-      for (int i = j - 1; i >= 0; --i) {
-        T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-        int k = i + 1;
-        for (; k + 3 <= j; k += 4) {
-          a0 += Dm[i * kLdS + k] * Ui[k * kLdS + j];
-          a1 += Dm[i * kLdS + k + 1] * Ui[(k + 1) * kLdS + j];
-          a2 += Dm[i * kLdS + k + 2] * Ui[(k + 2) * kLdS + j];
-          a3 += Dm[i * kLdS + k + 3] * Ui[(k + 3) * kLdS + j];
-        }
-        for (; k <= j; ++k) a0 += Dm[i * kLdS + k] * Ui[k * kLdS + j];
-        Ui[i * kLdS + j] = -((a0 + a1) + (a2 + a3)) / Dm[i * kLdS + i];
-      }
-    }
-  }
-  __syncthreads();
-  for (int e = tid; e < 64 * 64; e += kThreads) {
-    const int r = e >> 6, c = e & 63;
-    if (r < nb && c < nb) {
-      F[(int64_t)(p0 + r) * ldf + p0 + c] = Dm[r * kLdS + c];
-      SQ[(int64_t)(p0 + r) * ldn + p0 + c] = r > c ? Li[r * kLdS + c] : Ui[r * kLdS + c];
-    }
-  }
-}
-
-template <typename T>
 __global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, int p0,
                         int inst_base) {
   extern __shared__ unsigned char smem_raw[];
@@ -740,7 +659,8 @@ __device__ __forceinline__ void front_x_block(const T* Q, const T* Qt, int ldq, 
 // exchange slots alternate between two sets so that one barrier per step
 // orders every write after the previous step's reads.
 template <typename T, int G>
-__device__ __forceinline__ void front_lu(const T* Dm, T* Q, T* Qt, T* ex, int n, int ldq, int* status) {
+__device__ __forceinline__ void front_lu(const T* Dm, T* Q, T* Qt, T* ex, int n, int ldq, int* status,
+                                         T* LUo = nullptr) {
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   T A[G][G], X[G][G], Z[G][G];
 #pragma unroll
@@ -826,7 +746,43 @@ __device__ __forceinline__ void front_lu(const T* Dm, T* Q, T* Qt, T* ex, int n,
           Q[j * ldq + i] = Z[a][b];
           Qt[i * ldq + j] = Z[a][b];
         }
+        if (LUo) LUo[i * ldq + j] = A[a][b];
       }
+    }
+}
+
+// Diagonal block (p0 .. p0 + nb) of a blocked supernode: its LU back into the
+// front and strict_lower(inv(L)) + upper(inv(U)) into SQ, by the one-pass
+// register LU of the one-CTA fronts.
+template <typename T>
+__global__ void __launch_bounds__(256) k_diag(FactorDev D, T* fronts, T* factors, int64_t i0, int p0, int inst_base,
+                                              int* status) {
+  extern __shared__ unsigned char smem_raw[];
+  constexpr int ldq = kNB + 4;
+  T* Dm = reinterpret_cast<T*>(smem_raw);
+  T* Q = Dm + kNB * ldq;
+  T* Qt = Q + kNB * ldq;
+  T* ex = Qt + kNB * ldq;
+  const int s = D.items[i0 + blockIdx.x].x;
+  const int n = D.n[s];
+  const int nb = min(kNB, n - p0);
+  const int ldf = D.ldf[s], ldn = D.ldn[s];
+  T* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s] + (int64_t)p0 * ldf + p0;
+  T* SQ = factors + (int64_t)(inst_base + blockIdx.y) * D.fac_size + D.fac_off[s] + (int64_t)p0 * ldn + p0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int r = warp; r < nb; r += kThreads / 32)
+    for (int c = lane; c < nb; c += 32) cp_async_elem(Dm + r * ldq + c, F + (int64_t)r * ldf + c);
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  if (nb <= 16) front_lu<T, 1>(Dm, Q, Qt, ex, nb, ldq, status, Dm);
+  else if (nb <= 32) front_lu<T, 2>(Dm, Q, Qt, ex, nb, ldq, status, Dm);
+  else if (nb <= 48) front_lu<T, 3>(Dm, Q, Qt, ex, nb, ldq, status, Dm);
+  else front_lu<T, 4>(Dm, Q, Qt, ex, nb, ldq, status, Dm);
+  __syncthreads();
+  for (int r = warp; r < nb; r += kThreads / 32)
+    for (int c = lane; c < nb; c += 32) {
+      F[(int64_t)r * ldf + c] = Dm[r * ldq + c];
+      SQ[(int64_t)r * ldn + c] = Q[r * ldq + c];
     }
 }
 
@@ -1308,7 +1264,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   const int n_inst = n_active * f->n_bins;
   const size_t sm_gemm = 2 * 16 * kLdS * sizeof(T);
   const size_t sm_inv = sm_gemm + 64 * kLdS * sizeof(T);
-  const size_t sm_diag = 3 * 64 * kLdS * sizeof(T);
+  const size_t sm_diag = (3 * kNB * (kNB + 4) + 512) * sizeof(T);
   const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
   { int _r = allow_max_smem((const void*)k_schur<T>); if (_r) return _r; }
   bool use_tc = false;
