@@ -63,24 +63,32 @@ struct LdS {  // operand held in shared memory (ld kLdS)
   }
 };
 
+// acc (64 x 64, 4 x 4 per thread) += A (64 x K) B (K x 64) in 16-deep slabs
+// staged through shared memory; the next slab's operands are loaded into
+// registers while the current slab is multiplied.
 template <typename T, class LA, class LB>
 __device__ __forceinline__ void mma_tile(T (&acc)[4][4], int K, const LA& la, const LB& lb, T* As,
                                          T* Bs) {
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T ra[4], rb[4];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * kThreads;
+      ra[q] = la(e >> 4, k0 + (e & 15));
+      rb[q] = lb(k0 + (e >> 6), e & 63);
+    }
+  };
+  if (K > 0) fetch(0);
   for (int k0 = 0; k0 < K; k0 += 16) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      int e = tid + q * kThreads;
-      int r = e >> 4, kk = e & 15;
-      As[kk * kLdS + r] = la(r, k0 + kk);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int e = tid + q * kThreads;
-      int kk = e >> 6, c = e & 63;
-      Bs[kk * kLdS + c] = lb(k0 + kk, c);
+      const int e = tid + q * kThreads;
+      As[(e & 15) * kLdS + (e >> 4)] = ra[q];
+      Bs[(e >> 6) * kLdS + (e & 63)] = rb[q];
     }
     __syncthreads();
+    if (k0 + 16 < K) fetch(k0 + 16);
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
       T a[4], b[4];
@@ -492,12 +500,14 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
   T acc[4][4];
   zero_acc(acc);
   if (kind == 0) {
-    // Linv block (t, jb): -Linv_tt * sum_{k=jb}^{t-1} L_tk Linv_k,jb
-    const int r0 = 64 * t, h = min(64, n - r0), c0 = 64 * jb;
-    for (int k = jb; k < t; ++k) {
-      Ld<T> A{F + (int64_t)r0 * ldf + 64 * k, ldf, h, 64, 0, 0};
-      Ld<T> B{SQ + (int64_t)(64 * k) * ldn + c0, ldn, 64, 64, k == jb ? 1 : 0, 0};
-      mma_tile(acc, 64, A, B, As, Bs);
+    // Linv block (t, jb): -Linv_tt * sum_{k=jb}^{t-1} L_tk Linv_k,jb, the sum as
+    // one product over the contiguous columns 64 jb .. 64 t of L and rows of
+    // Linv (the unit-lower mask only bites in the first, diagonal block)
+    const int r0 = 64 * t, h = min(64, n - r0), c0 = 64 * jb, K = 64 * (t - jb);
+    {
+      Ld<T> A{F + (int64_t)r0 * ldf + c0, ldf, h, K, 0, 0};
+      Ld<T> B{SQ + (int64_t)c0 * ldn + c0, ldn, K, 64, 1, 0};
+      mma_tile(acc, K, A, B, As, Bs);
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -516,12 +526,13 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
         if (r < h) SQ[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
       }
   } else {
-    // Uinv block (jb, t): -(sum_{k=jb}^{t-1} Uinv_jb,k U_kt) Uinv_tt
-    const int r0 = 64 * jb, c0 = 64 * t, w = min(64, n - c0);
-    for (int k = jb; k < t; ++k) {
-      Ld<T> A{SQ + (int64_t)r0 * ldn + 64 * k, ldn, 64, 64, k == jb ? 2 : 0, 0};
-      Ld<T> B{F + (int64_t)(64 * k) * ldf + c0, ldf, 64, w, 0, 0};
-      mma_tile(acc, 64, A, B, As, Bs);
+    // Uinv block (jb, t): -(sum_{k=jb}^{t-1} Uinv_jb,k U_kt) Uinv_tt, the sum as
+    // one product (the upper mask only bites in the first, diagonal block)
+    const int r0 = 64 * jb, c0 = 64 * t, w = min(64, n - c0), K = 64 * (t - jb);
+    {
+      Ld<T> A{SQ + (int64_t)r0 * ldn + r0, ldn, 64, K, 2, 0};
+      Ld<T> B{F + (int64_t)r0 * ldf + c0, ldf, K, w, 0, 0};
+      mma_tile(acc, K, A, B, As, Bs);
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
