@@ -34,7 +34,7 @@ namespace orbit {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kLdS = 65;
+constexpr int kLdS = 68;  // shared-memory tile stride (16-byte aligned rows)
 
 template <typename T>
 struct Ld {
@@ -53,6 +53,19 @@ struct Ld {
   }
 };
 
+// 4 consecutive elements from 16-byte aligned shared memory.
+template <typename T>
+__device__ __forceinline__ void lds4(const T* p, T (&v)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+}
+
 template <typename T>
 struct LdS {  // operand held in shared memory (ld kLdS)
   const T* p;
@@ -63,7 +76,8 @@ struct LdS {  // operand held in shared memory (ld kLdS)
   }
 };
 
-// acc (64 x 64, 4 x 4 per thread) += A (64 x K) B (K x 64) in 16-deep slabs
+// acc (64 x 64; thread (ty, tx) holds rows 4 ty + i, columns 4 tx + j) +=
+// A (64 x K) B (K x 64) in 16-deep slabs
 // staged through shared memory; the next slab's operands are loaded into
 // registers while the current slab is multiplied.
 template <typename T, class LA, class LB>
@@ -92,10 +106,8 @@ __device__ __forceinline__ void mma_tile(T (&acc)[4][4], int K, const LA& la, co
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
       T a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk * kLdS + ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk * kLdS + tx + 16 * j];
+      lds4(As + kk * kLdS + 4 * ty, a);
+      lds4(Bs + kk * kLdS + 4 * tx, b);
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -276,7 +288,7 @@ __global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, in
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        int r = ty + 16 * i, c = tx + 16 * j;
+        int r = 4 * ty + i, c = 4 * tx + j;
         if (r < nb && c < w) F[(int64_t)(p0 + r) * ldf + c0 + c] = acc[i][j];
       }
   } else {
@@ -288,7 +300,7 @@ __global__ void k_panel(FactorDev D, T* fronts, const T* factors, int64_t i0, in
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        int r = ty + 16 * i, c = tx + 16 * j;
+        int r = 4 * ty + i, c = 4 * tx + j;
         if (r < h && c < nb) F[(int64_t)(r0 + r) * ldf + p0 + c] = acc[i][j];
       }
   }
@@ -512,7 +524,7 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) Xs[(ty + 16 * i) * kLdS + tx + 16 * j] = acc[i][j];
+      for (int j = 0; j < 4; ++j) Xs[(4 * ty + i) * kLdS + 4 * tx + j] = acc[i][j];
     __syncthreads();
     zero_acc(acc);
     Ld<T> A{SQ + (int64_t)r0 * ldn + r0, ldn, h, h, 1, 0};
@@ -522,7 +534,7 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        int r = ty + 16 * i, c = tx + 16 * j;
+        int r = 4 * ty + i, c = 4 * tx + j;
         if (r < h) SQ[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
       }
   } else {
@@ -537,7 +549,7 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) Xs[(ty + 16 * i) * kLdS + tx + 16 * j] = acc[i][j];
+      for (int j = 0; j < 4; ++j) Xs[(4 * ty + i) * kLdS + 4 * tx + j] = acc[i][j];
     __syncthreads();
     zero_acc(acc);
     LdS<T> A{Xs, 64, w};
@@ -547,7 +559,7 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        int r = ty + 16 * i, c = tx + 16 * j;
+        int r = 4 * ty + i, c = 4 * tx + j;
         if (c < w) SQ[(int64_t)(r0 + r) * ldn + c0 + c] = -acc[i][j];
       }
   }
@@ -569,19 +581,6 @@ __global__ void k_inv(FactorDev D, const T* fronts, T* factors, int64_t i0, int 
 //   Lt [n][ldl]  F21^T, then Pb^T
 //   U  [n][ldl]  F12
 //   ex [2][4][64] exchange slots of the pivot steps
-
-// 4 consecutive elements from 16-byte aligned shared memory.
-template <typename T>
-__device__ __forceinline__ void lds4(const T* p, T (&v)[4]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-  } else {
-    const double2 a = *reinterpret_cast<const double2*>(p);
-    const double2 b = *reinterpret_cast<const double2*>(p + 2);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
-}
 
 // Asynchronous copy of one element from global to shared memory.
 template <typename T>
