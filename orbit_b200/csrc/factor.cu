@@ -1048,21 +1048,22 @@ __global__ void __launch_bounds__(256) k_tc_pack(FactorDev D, const float* front
   }
 }
 
-constexpr int kTcStages = 3;
+constexpr int kTcStages = 2;
 constexpr int kTcStageBytes = 4 * tc::kTileBytes;  // A hi, A lo, B hi, B lo
 constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 512;
 constexpr long long kTcWaitLimit = 1LL << 22;
 
 // One 128 x 128 output tile per CTA of job 0 (X, written only as the X and
 // X^T operand packs), 1 (Pb, into the factor storage and as the Pb operand
-// pack), 2 (Qr, into the factor storage) or 3 (F22 += Pb F12).  Two CTAs per SM (96 KB ring and 128 TMEM columns each) so that one
-// CTA's epilogue overlaps the other's main loop.  Warp 0 lane 0 streams the
-// k-blocks into a 3-stage ring, warp 1 lane 0 issues the MMAs, all four warps
+// pack), 2 (Qr, into the factor storage) or 3 (F22 += Pb F12).  Three CTAs per SM (64 KB ring and 128 TMEM columns each) so that one
+// CTA's epilogue overlaps the others' main loops (measured faster than two
+// CTAs with 3-stage rings).  Warp 0 lane 0 streams the k-blocks into a
+// 2-stage ring, warp 1 lane 0 issues the MMAs, all four warps
 // read the accumulator back (warp w owns TMEM lanes 32w..32w+31 = tile rows)
 // and stage it through shared memory so that the output goes row by row,
 // coalesced.  Every wait is bounded; on a timeout the CTA lets its copies
 // land, skips the update, raises ORBIT_ERR_TIMEOUT and frees its tensor memory.
-__global__ void __launch_bounds__(128, 2) k_gemm_tc(FactorDev D, float* fronts, float* factors, float* pack,
+__global__ void __launch_bounds__(128, 3) k_gemm_tc(FactorDev D, float* fronts, float* factors, float* pack,
                                                     int64_t i0, int inst_base, int* status) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t full[kTcStages], empty[kTcStages], done;
