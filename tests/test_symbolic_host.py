@@ -174,3 +174,56 @@ def test_config_shapes_fill():
     assert s0.lunz < 2.5e6
     assert s1.lunz < 60e6
     assert s1.info["max_front"] < 2048
+
+
+def _fused_count(sym, max_n=64):
+    """Supernodes the analysis hands to the one-CTA front kernel: pivots
+    0 < n <= max_n, an update set (m > 0), and the kernel's shared memory
+    (inverses and their transpose, both panels, the pivot exchange slots)
+    within 28,672 elements."""
+    n = sym.array("n").astype(np.int64)
+    m = sym.array("m").astype(np.int64)
+    ldq = (n + 3) // 4 * 4 + 4
+    ldl = (m + 3) // 4 * 4
+    elems = 2 * n * ldq + 2 * n * ldl + 512
+    return int(((m > 0) & (n > 0) & (n <= max_n) & (elems <= 28672)).sum())
+
+
+@pytest.mark.parametrize("env,max_n", [(None, 64), ("32", 32), ("0", 0)])
+def test_fused_front_selection(monkeypatch, env, max_n):
+    if env is None:
+        monkeypatch.delenv("ORBIT_B200_FUSED_MAX_N", raising=False)
+    else:
+        monkeypatch.setenv("ORBIT_B200_FUSED_MAX_N", env)
+    for shape, leaf in (((15, 72, 80), 80), ((8, 22, 26), 48)):
+        sym = Symbolic(*shape, leaf_cells=leaf)
+        assert sym.info["fused_fronts"] == _fused_count(sym, max_n)
+    if max_n == 64:
+        # at the benchmark shape the three deepest levels are one-CTA fronts
+        sym = Symbolic(15, 72, 80, leaf_cells=80)
+        lev = sym.array("level")
+        assert sym.info["fused_fronts"] == 1792
+        assert np.all(sym.array("n")[lev >= lev.max() - 2] <= 64)
+
+
+def test_front_algebra_through_inverse_of_f11():
+    """The one-CTA fronts and the tensor-core pipeline form the panels through
+    X = inv(U11) inv(L11) = inv(F11): Pb = -F21 X, Qr = -X F12, and the Schur
+    complement F22 + Pb F12; the blocked CUDA-core path forms L21 = F21 inv(U11),
+    U12 = inv(L11) F12, Pb = -L21 inv(L11), Qr = -inv(U11) U12 and F22 - L21 U12.
+    Both give the same factor blocks (the stored factor is the same whichever
+    kernel produced it)."""
+    rng = np.random.default_rng(7)
+    for n, m in ((1, 5), (17, 9), (48, 64), (64, 200)):
+        F = rng.standard_normal((n + m, n + m)) + 4.0 * (n + m) * np.eye(n + m)
+        F11, F12, F21, F22 = F[:n, :n], F[:n, n:], F[n:, :n], F[n:, n:]
+        Lw, U = np.eye(n), F11.copy()
+        for k in range(n):
+            Lw[k + 1:, k] = U[k + 1:, k] / U[k, k]
+            U[k + 1:, k:] -= np.outer(Lw[k + 1:, k], U[k, k:])
+        U = np.triu(U)
+        Li, Ui = np.linalg.inv(Lw), np.linalg.inv(U)
+        L21, U12 = F21 @ Ui, Li @ F12
+        X = Ui @ Li
+        for a, b in ((-L21 @ Li, -F21 @ X), (-Ui @ U12, -X @ F12), (F22 - L21 @ U12, F22 + (-F21 @ X) @ F12)):
+            assert np.abs(a - b).max() <= 1e-12 * max(1.0, np.abs(a).max())
