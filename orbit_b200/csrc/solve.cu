@@ -32,8 +32,15 @@ namespace {
 #ifndef ORBIT_SOLVE_THREADS
 #define ORBIT_SOLVE_THREADS 128
 #endif
+// CTAs per SM the chain kernels are compiled for, per precision: FP32 at 10
+// (48 registers) hides more of the per-task latency than at 8 (64 registers),
+// 4 % faster on a 12-orbit chain even with the few spills it costs; FP64
+// stays at 8, where the single-orbit FP64 solve is fastest
 #ifndef ORBIT_SOLVE_MINB
 #define ORBIT_SOLVE_MINB 8
+#endif
+#ifndef ORBIT_SOLVE_MINB_FP32
+#define ORBIT_SOLVE_MINB_FP32 10
 #endif
 constexpr int kSolveThreads = ORBIT_SOLVE_THREADS;
 constexpr int kMaxPhases = 96;  // 2 x tree levels
@@ -425,7 +432,7 @@ __device__ void bwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain(ChainDev<T> D) {
+__global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MINB_FP32 : ORBIT_SOLVE_MINB) k_chain(ChainDev<T> D) {
   extern __shared__ unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);      // kWarps * 32
   T* vec = red + kWarps * 32;                    // front-sized vector
@@ -621,7 +628,7 @@ __device__ __forceinline__ void grouped_rows_multi(int r0, int r1, int wid, int 
   } while (0)
 
 template <typename T, int K>
-__global__ void __launch_bounds__(kSolveThreads, ORBIT_SOLVE_MINB) k_chain_multi(ChainDev<T> D, int vcap) {
+__global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MINB_FP32 : ORBIT_SOLVE_MINB) k_chain_multi(ChainDev<T> D, int vcap) {
   extern __shared__ unsigned char smem_raw[];
   T* vbuf = reinterpret_cast<T*>(smem_raw);  // K vectors of vcap
   __shared__ int s_task;
