@@ -227,3 +227,31 @@ def test_front_algebra_through_inverse_of_f11():
         X = Ui @ Li
         for a, b in ((-L21 @ Li, -F21 @ X), (-Ui @ U12, -X @ F12), (F22 - L21 @ U12, F22 + (-F21 @ X) @ F12)):
             assert np.abs(a - b).max() <= 1e-12 * max(1.0, np.abs(a).max())
+
+
+def test_one_pass_lu_with_inverses():
+    """The pivot steps of the one-CTA fronts (and of the blocked path's
+    diagonal blocks), restated: step k publishes row k of A, X, Z and column
+    k of A; rows i > k then apply A(i, j) -= l_i A(k, j) (j > k, l_i =
+    A(i, k) / A(k, k) stored at j = k), X(i, :) -= l_i X(k, :) and
+    Z(i, :) -= A(k, i) Z(k, :) / A(k, k), while row k of Z is scaled by
+    1 / A(k, k).  At the end A holds the unit-lower L and U, X = inv(L) and
+    Z = inv(U)^T."""
+    rng = np.random.default_rng(11)
+    for n in (1, 5, 16, 33, 64):
+        F = rng.standard_normal((n, n)) + 2.0 * n * np.eye(n)
+        A, X, Z = F.copy(), np.eye(n), np.eye(n)
+        for k in range(n):
+            rp = 1.0 / A[k, k]
+            pr, lc, xr, zr = A[k].copy(), A[:, k].copy(), X[k].copy(), Z[k].copy() * rp
+            for i in range(k + 1, n):
+                l = lc[i] * rp
+                A[i, k + 1:] -= l * pr[k + 1:]
+                A[i, k] = l
+                X[i] -= l * xr
+                Z[i] -= pr[i] * zr
+            Z[k] = zr
+        L, U = np.tril(A, -1) + np.eye(n), np.triu(A)
+        assert np.abs(L @ U - F).max() <= 1e-12 * np.abs(F).max()
+        assert np.abs(X - np.linalg.inv(L)).max() <= 1e-12
+        assert np.abs(Z.T - np.linalg.inv(U)).max() <= 1e-12 * np.abs(np.linalg.inv(U)).max()
