@@ -1,0 +1,62 @@
+"""The oracle's marginal FCT outer solve (restating orbit/modes/marginal.py:627-720),
+pinned on the CPU on a tiny grid.
+
+The deferred correction delta_c = K delta_c + b is linear: b is the orbit of
+the perturbation's forcing, K v the orbit of the extra right-hand sides
+-L_AD[tau] v[tau + 1].  Built column by column, (I - K) x = b can be solved
+densely; the oracle's GMRES result must match it, satisfy the fixed point to
+its tolerance, and reduce to the plain orbit solve when L_AD vanishes.
+"""
+import numpy as np
+import scipy.sparse as sp
+
+from oracle import assembly, fct as ofct, orbit as oorbit
+from orbit_b200 import synthetic
+
+NZ, NY, NX = 3, 4, 5
+N = NZ * NY * NX
+
+
+def _setup():
+    met = synthetic.make_met(9, NZ, NY, NX, cmfmc_frac=0.3)
+    spc = synthetic.make_species(31, NZ, NY, NX)
+    d = spc.sink_diag(met)
+    lus = [oorbit.factor_one_bin(assembly.species_operator(assembly.transport_block(met[t]), d[t]))
+           for t in range(8)]
+    base, _ = oorbit.solve_orbit_one_species(lus, list(spc.emis), tol=1e-13)
+    LAD = [ofct.fct_linear_operator(met[t], np.asarray(base[t + 1]), 10800.0) for t in range(8)]
+    dE = np.zeros_like(np.asarray(spc.emis))
+    dE[:, : NY * NX] = 0.1 * np.asarray(spc.emis)[:, : NY * NX]  # perturbed surface layer
+    return lus, LAD, dE
+
+
+def _orbit(lus, forcing):
+    orb, _ = oorbit.solve_orbit_one_species(lus, forcing, tol=1e-14)
+    return np.concatenate([np.asarray(o) for o in orb])
+
+
+def test_outer_solve_matches_dense_fixed_point():
+    lus, LAD, dE = _setup()
+    orbs, iters, rel = oorbit.fct_outer_solve([lus], [list(dE)], [LAD], tol=1e-14, rel_tol=1e-11, max_iters=60)
+    x = np.concatenate([np.asarray(o) for o in orbs[0]])
+    assert rel < 1e-8 and iters > 0
+    b = _orbit(lus, list(dE))
+
+    def K(v):
+        vv = v.reshape(9, N)
+        return _orbit(lus, [-(LAD[t] @ vv[t + 1]) for t in range(8)])
+
+    n = b.size
+    Km = np.stack([K(np.eye(n)[:, j]) for j in range(n)], axis=1)
+    xd = np.linalg.solve(np.eye(n) - Km, b)
+    assert np.abs(x - xd).max() <= 1e-7 * np.abs(xd).max()
+
+
+def test_outer_solve_without_coupling_is_the_plain_orbit():
+    lus, LAD, dE = _setup()
+    zero = [sp.csc_matrix((N, N)) for _ in range(8)]
+    orbs, _, rel = oorbit.fct_outer_solve([lus], [list(dE)], [zero], tol=1e-14, rel_tol=1e-10)
+    x = np.concatenate([np.asarray(o) for o in orbs[0]])
+    want = _orbit(lus, list(dE))
+    assert np.abs(x - want).max() <= 1e-10 * np.abs(want).max()
+    assert rel < 1e-10
