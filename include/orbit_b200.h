@@ -77,6 +77,11 @@ typedef struct {
   const double* lat;      /* (ny,) degrees */
   double dlat, dlon;      /* degrees */
   int split;              /* has_split_fluxes */
+  int pressure_form;      /* 1 when GridData.concentration_state is False: the
+                             transported variable is the mixing ratio, the state
+                             weights are 1 and the transport block is not put in
+                             concentration form (operator.py:341, fct.py:451-454,
+                             operator.py:626); 0 (default) for the concentration form */
 } orbit_met_t;
 
 /* Symbolic analysis of one (nz, ny, nx) domain: geometric nested dissection
@@ -129,6 +134,60 @@ int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int6
 int orbit_assemble_transport(int nz, int ny, int nx, const orbit_met_t* met,
                              double* T_stencil, double* rowsum, orbit_stream_t stream);
 
+/* Per-cell species fields of one bin for the species operators (device
+ * pointers; (nz, ny, nx) doubles unless noted; NULL where marked optional).
+ * Field meaning follows GridData (orbit/core/grid_data.py:19-215). */
+typedef struct {
+  const double* Dz;
+  const double* particle_dry_dep;  /* dry-deposition velocities (m/s); layer 0 is read */
+  const double* nh3_dry_dep;
+  const double* so2_dry_dep;
+  const double* nox_dry_dep;
+  const double* hno3_dry_dep;      /* optional: 3 cm/s at the surface when NULL */
+  const double* o3_dry_dep;        /* optional: 0.4 cm/s over land, 0.05 over water */
+  const double* is_land;           /* optional (ny, nx): land everywhere when NULL */
+  const double* voc_dry_dep;       /* optional: 0.1 cm/s organic vapour when NULL */
+  const double* particle_wet_dep;  /* wet-deposition rates (1/s) */
+  const double* other_gas_wet_dep;
+  const double* so2_wet_dep;
+  const double* nh_part;           /* TotalNH particle fraction (marginal or equilibrium, chosen by the caller) */
+  const double* no3_part;          /* optional TotalNO3 particle fraction: 0 when NULL */
+  const double* fp_vbs;            /* optional (5, nz, ny, nx) VBS particle fractions, bins C01..C1000 */
+  const double* fp_vbs_surface;    /* optional (5, ny, nx) */
+  const double* j_no2;             /* optional photolysis frequency for the SOA photolytic sink */
+  double a_photo;                  /* its scaling A_PHOTO (0 = off) */
+  const double* so2_ox;            /* optional SO2 -> pSO4 rate (1/s): 0 when NULL */
+  const double* nox_ox;            /* optional NOx -> TotalNO3 rate */
+  const double* o3_loss;           /* optional O3 chemistry loss */
+  const double* co_loss;           /* optional CO chemistry loss */
+  const double* archive_oh;        /* optional OH (molec/cm3): VBS aging when non-NULL */
+  double k_age;                    /* aging rate constant (cm3/molec/s) */
+  double aging_gain;               /* mass gained by the next-lower bin per unit aged */
+} orbit_species_fields_t;
+
+/* K1b: the 14 species' diagonal sink rates d_s (wet deposition + surface
+ * dry-deposition velocity / Dz + SOA photolysis + first-order chemistry
+ * losses) and the diagonals of the six source couplings K[(target, source)]
+ * (pSO4<-SO2, TotalNO3<-NOx, and the VBS aging cascade C100<-C1000,
+ * C10<-C100, C1<-C10, C01<-C1), for one bin.  d: device (14, N); k_src:
+ * device (6, N) or NULL, in that coupling order (rows of inactive couplings
+ * are zero).  Replaces the diagonal parts of assemble_species_operators
+ * (orbit/core/operator.py:371-595): assemble_deposition
+ * (orbit/core/deposition.py:101-146, 263-360), the SO2 oxidation blocks
+ * (orbit/core/chemistry.py:13-47) and the VBS aging blocks. */
+int orbit_species_diagonals(int nz, int ny, int nx, const orbit_species_fields_t* fields, double* d,
+                            double* k_src, orbit_stream_t stream);
+
+/* Coupled right-hand sides of one target species for 8 bins:
+ * out[tau] = e[tau] - sum_q kdiag[q][tau] * c_q[tau + shift_q] (c_q a source
+ * orbit, (9, N) device; shift 0 = start-of-bin, 1 = end-of-bin coupling;
+ * kdiag (n_src, 8, N) device; e, out (8, N) device, out may alias e).
+ * Replaces the K @ c_src products of solve_orbit_all_species
+ * (orbit/core/orbit.py:249-307) for the diagonal K-blocks of
+ * assemble_species_operators. */
+int orbit_source_coupling(int64_t N, int n_src, const double* const* c_src, const int* shift,
+                          const double* kdiag, const double* e, double* out, orbit_stream_t stream);
+
 /* K7: air-mass-balance row sums |T rho / rho| per day over laterally
  * interior cells for nbins stencils; writes the interior (nz-1 layers) and
  * top-layer magnitudes to out_interior / out_top (device, nbins*(nz-1)*(ny-2)*(nx-2)
@@ -143,6 +202,35 @@ int orbit_mass_balance_rows(int nz, int ny, int nx, int nbins, const double* con
  * Replaces compute_horizontal_fct_source (orbit/core/fct.py:459-492). */
 int orbit_fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
                      const double* c, double dt, int limited, double* d, orbit_stream_t stream);
+
+/* The 7-D ISORROPIA lookup table on the device: seven ascending axes (total
+ * SO4, total NH, total NO3, crustal Ca, sea-salt Na in ug/m3, T in K, RH in
+ * 0-1; device doubles, at least two points each) and up to four float32
+ * fields of shape n[0] x ... x n[6], C order (f_nh4, f_no3, aerosol_water,
+ * ph; NULL where not loaded). */
+typedef struct {
+  const double* axis[7];
+  int n[7];
+  const float* field[4];
+} orbit_lut_t;
+
+/* Query the LUT at n_pts points (pts: device (7, n_pts), one row per axis):
+ * multilinear interpolation, linear extrapolation from the edge cells, in
+ * double precision; out: device (4, n_pts) = clip(f_nh4, 0, 1),
+ * clip(f_no3, 0, 1), max(aerosol_water, 0), ph (NaN for fields not loaded).
+ * Replaces IsorropiaLUT.query (orbit/core/isorropia_lut.py:116-147, scipy
+ * RegularGridInterpolator "linear", fill_value None). */
+int orbit_lut_query(const orbit_lut_t* lut, int64_t n_pts, const double* pts, double* out, orbit_stream_t stream);
+
+/* out[i] = x_i . y for m <= 16 device vectors of n doubles (x: host array of
+ * device pointers; out: host, m doubles; synchronizes the stream).  With
+ * orbit_vec_combine, the device side of the Anderson step of the closure loop
+ * (AndersonAccelerator.update, orbit/core/closure_iteration.py:568-694). */
+int orbit_vec_dots(int64_t n, int m, const double* const* x, const double* y, double* out, orbit_stream_t stream);
+/* y = beta y + sum_i coef[i] x_i for m <= 16 device vectors (coef: host; y may
+ * be one of the x_i). */
+int orbit_vec_combine(int64_t n, int m, const double* coef, const double* const* x, double beta, double* y,
+                      orbit_stream_t stream);
 
 /* Frozen-gain FCT tangent-linear operator L_AD of n_vec baseline
  * concentrations c_base (device, n_vec x N): per face the gain C * beta of the
@@ -172,8 +260,11 @@ int orbit_stencil_apply(int nz, int ny, int nx, int n_vec, const double* stencil
  * doubles (24 MiB) that every GPU loading this library holds until exit, so
  * n_vec*nz*ny*nx must be <= 1,048,576 (larger requests return ORBIT_ERR_ARG).
  * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array, so calls
- * that overlap on the GPU (different streams or threads) race: serialize them. */
+ * first call before any stream capture.  The address is cached per device
+ * ordinal for the life of the process and does not survive a cudaDeviceReset
+ * (or any teardown of the device's primary context): do not call this entry
+ * point after one.  All calls share the array, so calls that overlap on the
+ * GPU (different streams or threads) race: serialize them. */
 int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec,
                              const double* c, double dt, int limited, double* d,
                              orbit_stream_t stream);

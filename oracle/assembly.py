@@ -235,9 +235,12 @@ def cmfmc_transport(g):
     return coo.csc()
 
 
-def transport_block(g, concentration_form=True):
-    """T = T_hcd + T_vadv + T_vdiff + T_conv, then diag(rho) T diag(1/rho)
-    (operator.py:281-353)."""
+def transport_block(g, concentration_form=None):
+    """T = T_hcd + T_vadv + T_vdiff + T_conv, then diag(rho) T diag(1/rho) when
+    the grid is in concentration form (operator.py:281-353, the
+    ``concentration_state`` switch at operator.py:341)."""
+    if concentration_form is None:
+        concentration_form = bool(getattr(g, "concentration_state", True))
     T = horizontal_convdiff(g) + vertical_advection(g) + vertical_diffusion(g) + cmfmc_transport(g)
     if concentration_form:
         rho = g.rho().reshape(-1)
@@ -261,7 +264,7 @@ def mass_balance_diagnostics(grids):
     ri_l, rt_l, per = [], [], []
     for g in grids:
         T = transport_block(g)
-        w = g.rho().reshape(-1)
+        w = g.state_weights().reshape(-1)  # rho, or 1 in the pressure form (operator.py:626)
         r = (np.asarray(T @ w).ravel() / w).reshape(nz, ny, nx) * DAY
         r = np.where(inner, r, np.nan)
         ri_l.append(r[:-1].ravel())

@@ -140,8 +140,9 @@ def _zalesak(g, c, faces, dt):
 
 
 def fct_source(g, c_flat, dt, limited=True):
-    """d_AD = rho * (-div(C (.) A)) on x = c/rho (fct.py:459-492)."""
-    rho = g.rho().reshape(-1)
+    """d_AD = rho * (-div(C (.) A)) on x = c/rho (fct.py:459-492); rho is the
+    state weight, 1 in the pressure form (_state_weights, fct.py:451-456)."""
+    rho = g.state_weights().reshape(-1)
     c = (np.asarray(c_flat, dtype=np.float64) / rho).reshape(g.nz, g.ny, g.nx)
     faces = _faces(g, c)
     Cx, Cy = _zalesak(g, c, faces, dt) if limited else (None, None)
@@ -152,7 +153,7 @@ def fct_linear_operator(g, c_base_flat, dt):
     """Frozen-gain 5-point L_AD with L_AD c_base = -d_AD(c_base) (fct.py:495-572)."""
     nz, ny, nx = g.nz, g.ny, g.nx
     N = nz * ny * nx
-    rho = g.rho().reshape(-1)
+    rho = g.state_weights().reshape(-1)
     c = (np.asarray(c_base_flat, dtype=np.float64) / rho).reshape(nz, ny, nx)
     idx = np.arange(N).reshape(nz, ny, nx)
     faces = _faces(g, c)

@@ -14,6 +14,7 @@ reference's documented no-UMFPACK path (SciPy SuperLU, COLAMD):
 * ``gradient_per_emission_bin``               orbit/core/orbit_adjoint.py:147-153
 * the FCT deferred-correction schedule        orbit/cli.py:1204-1241
 * the marginal FCT outer GMRES                orbit/modes/marginal.py:627-720
+* the adjoint FCT outer GMRES                 orbit/modes/adjoint.py:521-566, 814-960
 """
 from __future__ import annotations
 
@@ -179,3 +180,46 @@ def fct_outer_solve(lus_per_orbit, e_lists, L_AD, tol=1e-8, rel_tol=2e-3, max_it
     rel = float(np.abs(g - x).max() / max(np.abs(g).max(), 1e-30))
     orbits = [list(v) for v in g.reshape(n, N_BINS + 1, N)]
     return orbits, len(hist), rel
+
+
+def fct_adjoint_outer_solve(lus_per_orbit, R_lists, L_AD, tol=1e-8, rel_tol=2e-3, max_iters=40, dtau=DTAU):
+    """Adjoint FCT outer solve (orbit/modes/adjoint.py:521-566, 814-960): L_low^T
+    stays the factored propagator and the transposed anti-diffusive term enters
+    as a deferred receptor.  The co-forcing mu_tau = lambda_tau - R_tau (R the
+    effective receptor) satisfies the affine fixed point mu = K mu + b: b is the
+    low-order adjoint's mu, and K mu the mu of the adjoint solve whose receptor
+    adds nu_sigma = -dtau L_AD[sigma-1]^T mu[sigma-1] (bins mod 8; L_AD[tau]
+    frozen at the baseline's end-of-bin c[tau+1]).  Solved as GMRES on
+    (I - K) mu = b over all orbits flattened (x0 = b, atol = 0.3 rel_tol ||b||,
+    restart min(max_iters, 30)), then one final pass at the solution.  Returns
+    (adjoint orbits per orbit as 9 arrays, effective receptors per orbit as 8
+    arrays, outer iterations, rel_final = max|g(x) - x| / max|g(x)|)."""
+    n = len(lus_per_orbit)
+    N = lus_per_orbit[0][0].shape[0]
+
+    def recep_of(mu):
+        mm = mu.reshape(n, N_BINS, N)
+        return [[-dtau * (L_AD[o][(t - 1) % N_BINS].T @ mm[o][(t - 1) % N_BINS]) for t in range(N_BINS)]
+                for o in range(n)]
+
+    def inner(extra):
+        mus, lams, Rs = [], [], []
+        for o in range(n):
+            R = [R_lists[o][t] + (extra[o][t] if extra is not None else 0.0) for t in range(N_BINS)]
+            lam, _ = solve_orbit_adjoint_one_species(lus_per_orbit[o], R, tol=tol)
+            mus.append(np.concatenate([lam[t] - R[t] for t in range(N_BINS)]))
+            lams.append(lam)
+            Rs.append(R)
+        return np.concatenate(mus), lams, Rs
+
+    b, _, _ = inner(None)
+    op = spla.LinearOperator((b.size, b.size), matvec=lambda v: v - (inner(recep_of(v))[0] - b),
+                             dtype=np.float64)
+    restart = min(max_iters, 30)
+    hist = []
+    x, _ = spla.gmres(op, b, x0=b.copy(), rtol=1e-30, atol=0.3 * rel_tol * np.linalg.norm(b), restart=restart,
+                      maxiter=max(1, -(-max_iters // restart)), callback=lambda r: hist.append(r),
+                      callback_type="pr_norm")
+    g, lams, Rs = inner(recep_of(x))
+    rel = float(np.abs(g - x).max() / max(np.abs(g).max(), 1e-30))
+    return lams, Rs, len(hist), rel

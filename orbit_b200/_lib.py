@@ -34,7 +34,22 @@ class MetT(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "dP", "Dz", "u", "v", "u_plus", "u_minus", "v_plus", "v_minus", "u_e", "u_plus_e",
         "v_n", "v_plus_n", "kxxyy", "kzz", "w_plus", "w_minus", "cmfmc", "kmu", "kmv", "lat")] + [
-        ("dlat", C.c_double), ("dlon", C.c_double), ("split", C.c_int)]
+        ("dlat", C.c_double), ("dlon", C.c_double), ("split", C.c_int), ("pressure_form", C.c_int)]
+
+
+class SpeciesFieldsT(C.Structure):
+    """orbit_species_fields_t (include/orbit_b200.h)."""
+    _fields_ = [(n, C.c_void_p) for n in (
+        "Dz", "particle_dry_dep", "nh3_dry_dep", "so2_dry_dep", "nox_dry_dep", "hno3_dry_dep", "o3_dry_dep",
+        "is_land", "voc_dry_dep", "particle_wet_dep", "other_gas_wet_dep", "so2_wet_dep", "nh_part",
+        "no3_part", "fp_vbs", "fp_vbs_surface", "j_no2")] + [("a_photo", C.c_double)] + [
+        (n, C.c_void_p) for n in ("so2_ox", "nox_ox", "o3_loss", "co_loss", "archive_oh")] + [
+        ("k_age", C.c_double), ("aging_gain", C.c_double)]
+
+
+class LutT(C.Structure):
+    """orbit_lut_t (include/orbit_b200.h)."""
+    _fields_ = [("axis", C.c_void_p * 7), ("n", C.c_int * 7), ("field", C.c_void_p * 4)]
 
 
 EXPORTS = {
@@ -54,6 +69,14 @@ EXPORTS = {
                                            C.c_void_p, C.c_void_p]),
     "orbit_mass_balance_rows": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p]),
+    "orbit_species_diagonals": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(SpeciesFieldsT), C.c_void_p,
+                                          C.c_void_p, C.c_void_p]),
+    "orbit_source_coupling": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
+    "orbit_lut_query": (C.c_int, [C.POINTER(LutT), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "orbit_vec_dots": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "orbit_vec_combine": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                    C.c_void_p]),
     "orbit_fct_source": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_int, C.c_void_p,
                                    C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_fct_linear_operator": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_double,

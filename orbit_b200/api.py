@@ -117,41 +117,18 @@ def fct_operators(mets: Sequence["device.MetDevice"], c_base: torch.Tensor, dtau
     return L
 
 
-def solve_marginal_fct(fb: "device.FactorBatch", mets: Sequence["device.MetDevice"], L_AD: torch.Tensor,
-                       E: torch.Tensor, tol: float = 1e-6, rel_tol: float = 2e-3, max_iters: int = 40,
-                       maxiter: int = 200, dtau: float = DTAU):
-    """Marginal FCT outer solve (marginal.py:627-720) for a batch of orbits on
-    the device.  The deferred correction delta_c = K delta_c + b (b the orbit of
-    the forcing E, K v the orbit of the extra right-hand sides
-    -L_AD[o][tau] v[o][tau+1]) is solved as restarted GMRES on (I - K) delta_c
-    = b over the whole batch (x0 = b, atol = 0.3 rel_tol ||b||, restart
-    min(max_iters, 30)); every application of K is one batched device solve of
-    all orbits.  A last pass at the solution returns consistent orbits.
-    Returns (orbits (n, 9, N), info dict)."""
-    n, N = E.shape[0], E.shape[-1]
-    g0 = mets[0]
-    nz, ny, nx = g0.nz, g0.ny, g0.nx
-    solves = [0]
-
-    def inner(extra):
-        orb, _ = fb.solve(E if extra is None else E + extra, tol=tol, maxiter=maxiter, dtau=dtau)
-        solves[0] += 1
-        return orb.reshape(-1)
-
-    def extra_of(v):
-        vv = v.reshape(n, N_BINS + 1, N)
-        ex = torch.empty((n, N_BINS, N), dtype=torch.float64, device=E.device)
-        for t in range(N_BINS):
-            ex[:, t] = device.stencil_apply(nz, ny, nx, L_AD[:, t], vv[:, t + 1].contiguous(), alpha=-1.0)
-        return ex
-
-    b = inner(None)
+def _outer_gmres(g_of, b: torch.Tensor, rel_tol: float, max_iters: int):
+    """Restarted GMRES (modified Gram-Schmidt, Givens) on (I - K) x = b for the
+    affine map g(x) = K x + b, x0 = b, atol = 0.3 rel_tol ||b||, restart
+    min(max_iters, 30) -- the outer solver of the marginal and adjoint FCT
+    corrections (marginal.py:697-720, adjoint.py:868-941).  Every application
+    of K is one batched device solve.  Returns (x, iterations, converged)."""
     bnorm = float(torch.linalg.norm(b))
     atol = 0.3 * rel_tol * bnorm
     restart = min(max_iters, 30)
 
     def matvec(v):
-        return v - (inner(extra_of(v)) - b)
+        return v - (g_of(v) - b)
 
     x = b.clone()
     iters, converged = 0, bnorm == 0.0
@@ -193,7 +170,83 @@ def solve_marginal_fct(fb: "device.FactorBatch", mets: Sequence["device.MetDevic
             x = x + float(y[i]) * V[i]
         if abs(gvec[k]) <= atol:
             converged = True
+    return x, iters, converged
+
+
+def solve_marginal_fct(fb: "device.FactorBatch", mets: Sequence["device.MetDevice"], L_AD: torch.Tensor,
+                       E: torch.Tensor, tol: float = 1e-6, rel_tol: float = 2e-3, max_iters: int = 40,
+                       maxiter: int = 200, dtau: float = DTAU):
+    """Marginal FCT outer solve (marginal.py:627-720) for a batch of orbits on
+    the device.  The deferred correction delta_c = K delta_c + b (b the orbit of
+    the forcing E, K v the orbit of the extra right-hand sides
+    -L_AD[o][tau] v[o][tau+1]) is solved as restarted GMRES on (I - K) delta_c
+    = b over the whole batch (x0 = b, atol = 0.3 rel_tol ||b||, restart
+    min(max_iters, 30)); every application of K is one batched device solve of
+    all orbits.  A last pass at the solution returns consistent orbits.
+    Returns (orbits (n, 9, N), info dict)."""
+    n, N = E.shape[0], E.shape[-1]
+    g0 = mets[0]
+    nz, ny, nx = g0.nz, g0.ny, g0.nx
+    solves = [0]
+
+    def inner(extra):
+        orb, _ = fb.solve(E if extra is None else E + extra, tol=tol, maxiter=maxiter, dtau=dtau)
+        solves[0] += 1
+        return orb.reshape(-1)
+
+    def extra_of(v):
+        vv = v.reshape(n, N_BINS + 1, N)
+        ex = torch.empty((n, N_BINS, N), dtype=torch.float64, device=E.device)
+        for t in range(N_BINS):
+            ex[:, t] = device.stencil_apply(nz, ny, nx, L_AD[:, t], vv[:, t + 1].contiguous(), alpha=-1.0)
+        return ex
+
+    b = inner(None)
+    x, iters, converged = _outer_gmres(lambda v: inner(extra_of(v)), b, rel_tol, max_iters)
     g = inner(extra_of(x))
     rel_final = float((g - x).abs().max() / max(float(g.abs().max()), 1e-30))
     info = {"outer_iters": iters, "inner_solves": solves[0], "rel_final": rel_final, "converged": converged}
     return g.reshape(n, N_BINS + 1, N), info
+
+
+def solve_adjoint_fct(fb: "device.FactorBatch", mets: Sequence["device.MetDevice"], L_AD: torch.Tensor,
+                      R: torch.Tensor, tol: float = 1e-6, rel_tol: float = 2e-3, max_iters: int = 40,
+                      maxiter: int = 200, dtau: float = DTAU):
+    """Adjoint FCT outer solve (adjoint.py:521-566, 814-960) for a batch of
+    receptor sets on the device.  L_low^T stays the factored propagator; the
+    transposed anti-diffusive term enters as a deferred receptor.  The
+    co-forcing mu_tau = lambda_tau - R_tau (R the effective receptor) solves
+    the affine fixed point mu = K mu + b: b is the low-order adjoint's mu, K mu
+    the mu of the adjoint solve whose receptor adds
+    nu_sigma = -dtau L_AD[sigma-1]^T mu[sigma-1] (bins mod 8; L_AD[tau] frozen
+    at the baseline's end-of-bin c[tau+1], the stencils of ``fct_operators``).
+    Restarted GMRES on (I - K) mu = b over the whole batch, every application
+    of K one batched transposed device solve, then a final pass at the
+    solution.  Returns (adjoint orbits (n, 9, N), effective receptors
+    (n, 8, N), info dict); dJ/de_tau = dtau (lambda_tau - R_tau) holds for them."""
+    n, N = R.shape[0], R.shape[-1]
+    g0 = mets[0]
+    nz, ny, nx = g0.nz, g0.ny, g0.nx
+    solves = [0]
+
+    def inner(nu):
+        Reff = R if nu is None else R + nu
+        lam, _ = fb.solve_adjoint(Reff, tol=tol, maxiter=maxiter)
+        solves[0] += 1
+        return (lam[:, :N_BINS] - Reff).reshape(-1), lam, Reff
+
+    def recep_of(mu):
+        mm = mu.reshape(n, N_BINS, N)
+        nu = torch.empty((n, N_BINS, N), dtype=torch.float64, device=R.device)
+        for t in range(N_BINS):
+            src = (t - 1) % N_BINS
+            nu[:, t] = device.stencil_apply(nz, ny, nx, L_AD[:, src], mm[:, src].contiguous(), alpha=-dtau,
+                                            trans=True)
+        return nu
+
+    b, _, _ = inner(None)
+    x, iters, converged = _outer_gmres(lambda v: inner(recep_of(v))[0], b, rel_tol, max_iters)
+    g, lam, Reff = inner(recep_of(x))
+    rel_final = float((g - x).abs().max() / max(float(g.abs().max()), 1e-30))
+    info = {"outer_iters": iters, "inner_solves": solves[0], "rel_final": rel_final, "converged": converged}
+    return lam, Reff, info

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "liborbit_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["symbolic.cpp", "capi.cu", "factor.cu", "solve.cu", "gmres.cu", "assemble.cu", "fct.cu"]
+SOURCES = ["symbolic.cpp", "capi.cu", "factor.cu", "solve.cu", "gmres.cu", "assemble.cu", "fct.cu", "species.cu", "closure.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -219,9 +219,12 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
     }
   }
   if (rowsum) rowsum[cell] = diag + oW + oE + oS + oN + oB + oT;
-  // ---- concentration form: off(c, nb) *= rho_c / rho_nb ----
+  // ---- concentration form: off(c, nb) *= rho_c / rho_nb (pressure-form
+  // grids keep the block as assembled, operator.py:341) ----
   const double rc = rho_of(dPc, Dzc);
-  auto sim = [&](double v, int64_t nb) { return v == 0.0 ? 0.0 : rc * v / rho_of(g.dP[nb], g.Dz[nb]); };
+  auto sim = [&](double v, int64_t nb) {
+    return (v == 0.0 || g.pressure_form) ? v : rc * v / rho_of(g.dP[nb], g.Dz[nb]);
+  };
   Tst[0 * NN + cell] = diag;
   Tst[1 * NN + cell] = i > 0 ? sim(oW, cell - 1) : 0.0;
   Tst[2 * NN + cell] = i < nx - 1 ? sim(oE, cell + 1) : 0.0;

@@ -1243,6 +1243,11 @@ __global__ void __launch_bounds__(128, 3) k_gemm_tc(FactorDev D, float* fronts, 
   } else if (threadIdx.x == 0) {
     raise_status(status, ORBIT_ERR_TIMEOUT);
   }
+  // On a timeout, MMAs already issued may still write this CTA's tensor
+  // memory: wait once more (bounded) for their commit before the columns are
+  // released.  The status word then carries ORBIT_ERR_TIMEOUT and the handle's
+  // factors are not to be used.
+  if (!ok) tc::mbar_wait(&done, 0, kTcWaitLimit);
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 1) tc::tmem_dealloc(tmem, 128);

@@ -26,7 +26,10 @@ struct FctGeom {
   double dt;
 };
 
+// State weight of a cell: rho = dP / (g Dz) in the concentration form, 1 in the
+// pressure form (_state_weights, fct.py:451-456).
 __device__ __forceinline__ double rho_at(const orbit_met_t& g, int64_t c) {
+  if (g.pressure_form) return 1.0;
   const double dP = g.dP[c], Dz = g.Dz[c];
   return (dP > 0.0 && Dz > 0.0) ? dP / (kGravity * Dz) : 1.0;
 }
@@ -279,8 +282,10 @@ int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const 
   dim3 g((unsigned)((N + 127) / 128), n_vec);
   k_fct_x<<<g, 128, 0, st>>>(G, c, x, N);
   note_launch();
-  if (limited) k_fct_ratio<<<g, 128, 0, st>>>(G, x, Rp, Rm, N);
-  note_launch();
+  if (limited) {
+    k_fct_ratio<<<g, 128, 0, st>>>(G, x, Rp, Rm, N);
+    note_launch();
+  }
   k_fct_div<<<g, 128, 0, st>>>(G, x, Rp, Rm, limited, d, N);
   note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
@@ -352,7 +357,10 @@ int fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec
   double* scratch = nullptr;
   {
     // The array's name is only a host-side stand-in for the symbol; its device
-    // address is looked up once per device, with that device current.
+    // address is looked up once per device, with that device current.  The
+    // cached address belongs to the device's current primary context: after a
+    // cudaDeviceReset the module may load elsewhere, so the entry point must
+    // not be called after one.
     std::lock_guard<std::mutex> lk(g_fct_scratch_mu);
     if (!g_fct_scratch_ptr[dev]) {
       void* p = nullptr;

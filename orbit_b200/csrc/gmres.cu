@@ -656,7 +656,12 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   const double fscale = trans ? 1.0 : dtau;
   std::vector<int> mv(f->n_orbits, 0), iters(f->n_orbits, 0), conv(f->n_orbits, 0), outer(f->n_orbits, 0);
   std::vector<double> rn(f->n_orbits, 0.0);
-  rc = chain_accurate(c, d_ids, n, f->E, fscale);
+  // s = sweep of the forcing from zero.  In the mixed forward solve s only
+  // sets the stopping tolerance (atol = tol ||s||; the block-cyclic refinement
+  // starts from the forcing itself), so one FP32 sweep is enough there: its
+  // norm is exact to ~1e-7 relative.  Every other path sweeps accurately.
+  if (c.mixed && !trans) rc = launch_chain(f, n, d_ids, 0, 0, 8, f->E, fscale, st);
+  else rc = chain_accurate(c, d_ids, n, f->E, fscale);
   if (rc) return rc;
   for (int o = 0; o < n; ++o) mv[o]++;
   k_lincomb<<<g, kVT, 0, st>>>(c.Sv, c.vs, one, f->X + outb * N, 9 * N, zero, nullptr, 0, d_ids, N);

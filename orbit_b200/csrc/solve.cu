@@ -20,10 +20,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
 #include "handles.h"
+#include "tc.cuh"
 
 namespace orbit {
 
@@ -437,7 +439,8 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
   T* red = reinterpret_cast<T*>(smem_raw);      // kWarps * 32
   T* vec = red + kWarps * 32;                    // front-sized vector
   __shared__ int s_task;
-  __shared__ int s_ok;
+  __shared__ int s_ok;   // status word clean at the claim
+  __shared__ int s_dep;  // dependency wait succeeded
   __shared__ int s_phase[kMaxPhases + 1];  // phase offsets x B
   const int tid = threadIdx.x;
   const int per_bin = D.items_per_bin * D.B;
@@ -519,11 +522,11 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
         else
           ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
       }
-      s_ok = ok;
+      s_dep = ok;
       __threadfence();
     }
     __syncthreads();
-    if (!s_ok) break;
+    if (!s_dep) break;
     if (!subtree) {
       if (fwd) fwd_node(D, o, tau, s, it.y, it.z, trans, vec, red);
       else bwd_node(D, o, tau, s, it.y, it.z, trans, vec, red);
@@ -631,8 +634,10 @@ template <typename T, int K>
 __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MINB_FP32 : ORBIT_SOLVE_MINB) k_chain_multi(ChainDev<T> D, int vcap) {
   extern __shared__ unsigned char smem_raw[];
   T* vbuf = reinterpret_cast<T*>(smem_raw);  // K vectors of vcap
+  T* red = vbuf + (int64_t)K * vcap;          // K x kWarps x 32 (transposed sweeps)
   __shared__ int s_task;
-  __shared__ int s_ok;
+  __shared__ int s_ok;   // status word clean at the claim
+  __shared__ int s_dep;  // dependency wait succeeded
   __shared__ int s_phase[kMaxPhases + 1];
   const int tid = threadIdx.x, warp = tid >> 5;
   const int per_bin = D.items_per_bin * D.B;
@@ -647,7 +652,7 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     if (t >= D.total || !s_ok) break;
     const int q = t / per_bin;
     const int r = t - q * per_bin;
-    const int tau = D.tau0 + q;
+    const int tau = D.trans ? (D.tau1 - 1 - q) : (D.tau0 + q);
     int lo = 0, hi = D.nphase;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
@@ -676,25 +681,146 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     }
     if (tid == 0) {
       bool ok = true;
-      if (kind == 0) {
+      if (kind == 0 || kind == 2) {
         for (int q2 = 0; q2 < 2 && ok; ++q2) {
           const int c = D.child[2 * s + q2];
           if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
         }
-        if (ok && tau > D.tau0)
+        if (ok && kind == 0 && tau > D.tau0)
           ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+        if (ok && kind == 2 && tau < D.tau1 - 1)
+          ok = wait_ge(cbase + ((tau + 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
       } else {
         const int par = D.parent[s];
         if (par < 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit);
         else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
       }
-      s_ok = ok;
+      s_dep = ok;
       __threadfence();
     }
     __syncthreads();
-    if (!s_ok) break;
+    if (!s_dep) break;
     const int n0pad = (n + 3) & ~3;
-    if (kind == 0) {
+    const int lane = tid & 31;
+    if (kind == 2) {
+      // transposed forward (U^T, then the update columns): gather over
+      // [0, min(r1, n)) and [max(r0, n), r1) as the forward rows do, then
+      // columns [r0, r1) of [upper(SQ) | Qr], each factor element used for
+      // the K vectors
+      const int lo_end = min(r1, n), hi0 = max(r0, n), w = n + m;
+      const int32_t* g0 = D.ginv + D.ginv_off[s];
+      const int32_t* g1 = g0 + w;
+      const int c0 = D.child[2 * s], c1 = D.child[2 * s + 1];
+      for (int k = 0; k < nk; ++k) {
+        T* vec = vbuf + k * vcap;
+        const double* Xin = D.X + ((int64_t)o[k] * 9 + tau + 1) * D.N;
+        const double* Ein = (D.E && tau + 1 < D.tau1) ? D.E + ((int64_t)o[k] * 8 + tau + 1) * D.N : nullptr;
+        const double* Wo = D.W + (int64_t)o[k] * D.w_size;
+        const double* W0 = c0 >= 0 ? Wo + D.woff[c0] : nullptr;
+        const double* W1 = c1 >= 0 ? Wo + D.woff[c1] : nullptr;
+        for (int i = tid; i < lo_end; i += kSolveThreads) {
+          double v = Xin[first + i];
+          if (Ein) v += D.escale * Ein[first + i];
+          const int u0 = g0[i], u1 = g1[i];
+          if (u0 >= 0) v += W0[u0];
+          if (u1 >= 0) v += W1[u1];
+          vec[i] = (T)v;
+        }
+        for (int i = hi0 + tid; i < r1; i += kSolveThreads) {
+          double v = 0.0;
+          const int u0 = g0[i], u1 = g1[i];
+          if (u0 >= 0) v += W0[u0];
+          if (u1 >= 0) v += W1[u1];
+          vec[i] = (T)v;
+        }
+      }
+      __syncthreads();
+      const T* Qr = SQ + (int64_t)(n + m) * ldn;
+      const int64_t woff = D.woff[s];
+      for (int cb = r0; cb < r1; cb += 32) {
+        const int c = cb + lane;
+        T acc[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] = T(0);
+        if (c < r1) {
+          if (c < n) {
+            for (int i = warp; i <= c; i += kWarps) {
+              const T x = __ldg(SQ + (int64_t)i * ldn + c);
+#pragma unroll
+              for (int k = 0; k < K; ++k)
+                if (k < nk) acc[k] = fma(x, vbuf[k * vcap + i], acc[k]);
+            }
+          } else {
+            const int u = c - n;
+            for (int i = warp; i < n; i += kWarps) {
+              const T x = __ldg(Qr + (int64_t)i * ldm + u);
+#pragma unroll
+              for (int k = 0; k < K; ++k)
+                if (k < nk) acc[k] = fma(x, vbuf[k * vcap + i], acc[k]);
+            }
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[(k * kWarps + warp) * 32 + lane] = acc[k];
+        __syncthreads();
+        if (warp == 0 && c < r1) {
+          for (int k = 0; k < nk; ++k) {
+            T sum = T(0);
+#pragma unroll
+            for (int w2 = 0; w2 < kWarps; ++w2) sum += red[(k * kWarps + w2) * 32 + lane];
+            if (c < n) D.Y[(int64_t)o[k] * D.N + first + c] = (double)sum;
+            else D.W[(int64_t)o[k] * D.w_size + woff + (c - n)] = (double)(vbuf[k * vcap + c] + sum);
+          }
+        }
+        __syncthreads();
+      }
+    } else if (kind == 3) {
+      // transposed backward (L^T with unit diagonal): columns [r0, r1) of
+      // [strict lower(SQ) ; Pb] against the own forward results and the
+      // ancestors' solution
+      const int32_t* ui = D.uidx + D.uoff[s];
+      for (int k = 0; k < nk; ++k) {
+        T* vec = vbuf + k * vcap;
+        const double* Yo = D.Y + (int64_t)o[k] * D.N;
+        const double* Xout = D.X + ((int64_t)o[k] * 9 + tau) * D.N;
+        for (int i = r0 + tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
+        for (int u = tid; u < m; u += kSolveThreads) vec[n0pad + u] = (T)Xout[ui[u]];
+      }
+      __syncthreads();
+      const T* Pb = SQ + (int64_t)n * ldn;
+      for (int cb = r0; cb < r1; cb += 32) {
+        const int c = cb + lane;
+        T acc[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] = T(0);
+        if (c < r1) {
+          for (int i = c + 1 + warp; i < n; i += kWarps) {
+            const T x = __ldg(SQ + (int64_t)i * ldn + c);
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k < nk) acc[k] = fma(x, vbuf[k * vcap + i], acc[k]);
+          }
+          for (int u = warp; u < m; u += kWarps) {
+            const T x = __ldg(Pb + (int64_t)u * ldn + c);
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k < nk) acc[k] = fma(x, vbuf[k * vcap + n0pad + u], acc[k]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[(k * kWarps + warp) * 32 + lane] = acc[k];
+        __syncthreads();
+        if (warp == 0 && c < r1) {
+          for (int k = 0; k < nk; ++k) {
+            T sum = vbuf[k * vcap + c];
+#pragma unroll
+            for (int w2 = 0; w2 < kWarps; ++w2) sum += red[(k * kWarps + w2) * 32 + lane];
+            D.X[((int64_t)o[k] * 9 + tau) * D.N + first + c] = (double)sum;
+          }
+        }
+        __syncthreads();
+      }
+    } else if (kind == 0) {
       // gather each right-hand side's vector over the range the rows read
       const int lo_end = min(r1, n), hi0 = max(r0, n), w = n + m;
       const int32_t* g0 = D.ginv + D.ginv_off[s];
@@ -766,6 +892,360 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     __syncthreads();
     if (tid == 0) {
       __threadfence();
+      red_release_add(cbase + (tau * 2 + ((kind == 0 || kind == 2) ? 0 : 1)) * D.nsuper + s, 1);
+    }
+  }
+}
+
+// ---- staged chain: factor rows moved to shared memory by the TMA engine ----
+//
+// Each task's factor rows are copied global -> shared memory with linear
+// bulk copies (cp.async.bulk, completing on an mbarrier, evict-first in L2)
+// that are issued before the task's dependency wait, so the factor stream
+// is in flight while the task waits for its predecessors and gathers its
+// right-hand side; the dense rows are then multiplied from shared memory.
+// A task's rows are moved in pieces that fit one half of a two-buffer stage:
+// the first two pieces are issued before the wait, each later piece as soon
+// as the buffer it reuses has been consumed.  Rows stage as they are used:
+// forward, row i < n of SQ keeps columns [0, pad4(i)) (the strictly lower
+// part, inv(L11)) and the Pb rows [n, n + m) are one contiguous block;
+// backward, row i keeps the SQ columns [i & ~3, ldn) (inv(U11)) followed by
+// the contiguous Qr rows of the piece.  Non-transposed sweeps only; K
+// right-hand sides per task when every solve slot shares one factor set.
+
+__device__ __forceinline__ int pad4i(int k) { return (k + 3) & ~3; }
+// sum_{k < i} pad4(k)
+__device__ __forceinline__ int64_t pad4_prefix(int i) {
+  if (i <= 1) return 0;
+  const int64_t a = i - 1, g = a >> 2, r = a & 3;
+  return 8 * g * (g + 1) + 4 * r * (g + 1);
+}
+// sum_{k < i} (k & ~3)
+__device__ __forceinline__ int64_t floor4_prefix(int i) {
+  const int64_t g = i >> 2, r = i & 3;
+  return 8 * g * (g - 1) + 4 * r * g;
+}
+// Staged elements of rows [0, i) of a task of the given kind (0 forward, 1 backward).
+__device__ __forceinline__ int64_t staged_prefix(int kind, int i, int n, int ldn, int ldm) {
+  if (kind == 0) return pad4_prefix(min(i, n)) + (int64_t)ldn * max(i - n, 0);
+  return (int64_t)(ldn + (ldm > 0 ? ldm : 0)) * i - floor4_prefix(i);
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                              uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          tc::smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(tc::smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Dot product of a shared-memory row segment (16-byte aligned at j = 0) with
+// K shared-memory vectors over [j0, j1): G lanes, four 16-byte loads in
+// flight per lane.
+template <typename T, int G, int K>
+__device__ __forceinline__ void dot_seg_smem(const T* a, const T* v, int vcap, int nk, int j0, int j1, int gl,
+                                             T (&acc)[K]) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::w;
+  const int ja = min((j0 + W - 1) / W * W, j1);
+  const int jb = max(ja, j1 / W * W);
+  for (int j = j0 + gl; j < ja; j += G) {
+    const T x = a[j];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) acc[k] = fma(x, v[k * vcap + j], acc[k]);
+  }
+  const V* a4 = reinterpret_cast<const V*>(a);
+  const int nv0 = ja / W, nv1 = jb / W;
+  for (int kk = nv0 + gl; kk < nv1; kk += 2 * G) {
+    const bool b1 = kk + G < nv1;
+    const V x0 = a4[kk];
+    V x1 = {};
+    if (b1) x1 = a4[kk + G];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) {
+        acc[k] += dot16(x0, v + k * vcap + kk * W);
+        if (b1) acc[k] += dot16(x1, v + k * vcap + (kk + G) * W);
+      }
+  }
+  for (int j = jb + gl; j < j1; j += G) {
+    const T x = a[j];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) acc[k] = fma(x, v[k * vcap + j], acc[k]);
+  }
+}
+
+struct StagePiece {
+  int a, b;  // rows [a, b) of the task
+};
+
+// Largest b in (a, r1] whose rows [a, b) stage in at most cap elements (every
+// single row fits a half stage by construction of cap).
+__device__ __forceinline__ int piece_end(int kind, int a, int r1, int n, int ldn, int ldm, int64_t cap) {
+  const int64_t base = staged_prefix(kind, a, n, ldn, ldm);
+  int lo = a + 1, hi = r1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (staged_prefix(kind, mid, n, ldn, ldm) - base <= cap) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Issue the bulk copies of rows [a, b) into `buf` (warp 0 only; lane 0 posts
+// the byte count first).
+template <typename T>
+__device__ __forceinline__ void issue_piece(const T* SQ, int kind, int a, int b, int n, int m, int ldn, int ldm,
+                                            T* buf, uint64_t* bar, uint64_t pol) {
+  const int lane = threadIdx.x & 31;
+  const int64_t base = staged_prefix(kind, a, n, ldn, ldm);
+  const int64_t total = staged_prefix(kind, b, n, ldn, ldm) - base;
+  if (lane == 0) {
+    fence_proxy_async_smem();
+    tc::mbar_arrive_expect_tx(bar, (uint32_t)(total * sizeof(T)));
+  }
+  __syncwarp();
+  if (kind == 0) {
+    // SQ rows [a, min(b, n)): columns [0, pad4(i))
+    const int sq_end = min(b, n);
+    for (int i = a + lane; i < sq_end; i += 32) {
+      const int len = pad4i(i);
+      if (len > 0)
+        bulk_g2s_hint(buf + (pad4_prefix(i) - pad4_prefix(a)), SQ + (int64_t)i * ldn, (uint32_t)(len * sizeof(T)),
+                      bar, pol);
+    }
+    const int pa = max(a, n), pb = max(b, n);
+    if (pb > pa && lane == 0) {
+      const int64_t off = pad4_prefix(sq_end) - pad4_prefix(min(a, n));
+      bulk_g2s_hint(buf + off, SQ + (int64_t)pa * ldn, (uint32_t)((int64_t)(pb - pa) * ldn * sizeof(T)), bar, pol);
+    }
+  } else {
+    // SQ rows [a, b): columns [i & ~3, ldn); then the Qr rows [a, b)
+    for (int i = a + lane; i < b; i += 32) {
+      const int c0 = i & ~3;
+      const int64_t off = (int64_t)(i - a) * ldn - (floor4_prefix(i) - floor4_prefix(a));
+      bulk_g2s_hint(buf + off, SQ + (int64_t)i * ldn + c0, (uint32_t)((ldn - c0) * sizeof(T)), bar, pol);
+    }
+    if (m > 0 && lane == 0) {
+      const int64_t off = (int64_t)(b - a) * ldn - (floor4_prefix(b) - floor4_prefix(a));
+      const T* Qr = SQ + (int64_t)(n + m) * ldn;
+      bulk_g2s_hint(buf + off, Qr + (int64_t)a * ldm, (uint32_t)((int64_t)(b - a) * ldm * sizeof(T)), bar, pol);
+    }
+  }
+}
+
+#ifndef ORBIT_STAGED_MINB
+#define ORBIT_STAGED_MINB 4
+#endif
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolveThreads, ORBIT_STAGED_MINB) k_chain_staged(ChainDev<T> D, int vcap,
+                                                                                   int half_elems) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* stage = reinterpret_cast<T*>(smem_raw);               // 2 x half_elems
+  T* vbuf = stage + 2 * (int64_t)half_elems;                // K vectors of vcap
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ int s_task;
+  __shared__ int s_ok;   // status word clean at the claim
+  __shared__ int s_dep;  // dependency wait succeeded
+  __shared__ int s_phase[kMaxPhases + 1];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int per_bin = D.items_per_bin * D.B;
+  for (int i = tid; i <= D.nphase; i += blockDim.x) s_phase[i] = D.phase_off[i] * D.B;
+  if (tid == 0) {
+    tc::mbar_init(&bars[0], 1);
+    tc::mbar_init(&bars[1], 1);
+    tc::fence_barrier_init();
+  }
+  __syncthreads();
+  const uint64_t pol = l2_evict_first_policy();
+  uint32_t par0 = 0, par1 = 0;  // next phase parity of each stage buffer
+  constexpr long long kStageWait = 1LL << 24;
+  for (;;) {
+    if (tid == 0) {
+      s_task = atomicAdd(D.task_counter, 1);
+      s_ok = ld_volatile(D.status) == 0;
+    }
+    __syncthreads();
+    const int t = s_task;
+    if (t >= D.total || !s_ok) break;
+    const int q = t / per_bin;
+    const int r = t - q * per_bin;
+    const int tau = D.tau0 + q;
+    int lo = 0, hi = D.nphase;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_phase[mid] <= r) lo = mid;
+      else hi = mid;
+    }
+    const int rr = r - s_phase[lo];
+    const int cnt = D.phase_off[lo + 1] - D.phase_off[lo];
+    const int gi = rr / cnt;
+    const int4 it = D.items[D.phase_off[lo] + (rr - gi * cnt)];
+    const int s = it.x, kind = it.w, r0 = it.y, r1 = it.z;
+    const int nk = K == 1 ? 1 : min(K, D.Borb - gi * K);
+    int o[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = D.orbit_ids[gi * K + (k < nk ? k : 0)];
+    int* cbase = D.counters + (int64_t)o[0] * 8 * 2 * D.nsuper;
+    const int n = D.n[s], m = D.m[s], first = D.first[s], ldn = D.ldn[s], ldm = D.ldm[s];
+    const int ldm_st = m > 0 ? ldm : 0;
+    const T* SQ = D.factors + ((int64_t)D.set_of[o[0]] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+    // ---- pieces 0 and 1 in flight before the dependency wait ----
+    int pa = r0, pb = piece_end(kind, r0, r1, n, ldn, ldm_st, half_elems);
+    int pc = pb < r1 ? piece_end(kind, pb, r1, n, ldn, ldm_st, half_elems) : pb;
+    if (warp == 0) {
+      issue_piece<T>(SQ, kind, pa, pb, n, m, ldn, ldm_st, stage, &bars[0], pol);
+      if (pc > pb) issue_piece<T>(SQ, kind, pb, pc, n, m, ldn, ldm_st, stage + half_elems, &bars[1], pol);
+    }
+    // ---- dependencies ----
+    if (tid == 0) {
+      bool ok = true;
+      if (kind == 0) {
+        for (int q2 = 0; q2 < 2 && ok; ++q2) {
+          const int c = D.child[2 * s + q2];
+          if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
+        }
+        if (ok && tau > D.tau0)
+          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+      } else {
+        const int par = D.parent[s];
+        if (par < 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit);
+        else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
+      }
+      s_dep = ok;
+      __threadfence();
+    }
+    __syncthreads();
+    if (!s_dep) {
+      // leave only once the copies this task issued have landed
+      if (tid == 0) {
+        tc::mbar_wait(&bars[0], par0, kStageWait);
+        if (pc > pb) tc::mbar_wait(&bars[1], par1, kStageWait);
+      }
+      __syncthreads();
+      break;
+    }
+    // ---- right-hand sides over the range the rows read ----
+    const int n0pad = (n + 3) & ~3;
+    if (kind == 0) {
+      const int lo_end = min(r1, n), hi0 = max(r0, n), w = n + m;
+      const int32_t* g0 = D.ginv + D.ginv_off[s];
+      const int32_t* g1 = g0 + w;
+      const int c0 = D.child[2 * s], c1 = D.child[2 * s + 1];
+      for (int k = 0; k < nk; ++k) {
+        T* vec = vbuf + k * vcap;
+        const double* Xin = D.X + ((int64_t)o[k] * 9 + tau) * D.N;
+        const double* Ein = D.E ? D.E + ((int64_t)o[k] * 8 + tau) * D.N : nullptr;
+        const double* Wo = D.W + (int64_t)o[k] * D.w_size;
+        const double* W0 = c0 >= 0 ? Wo + D.woff[c0] : nullptr;
+        const double* W1 = c1 >= 0 ? Wo + D.woff[c1] : nullptr;
+        for (int i = tid; i < lo_end; i += kSolveThreads) {
+          double v = Xin[first + i];
+          if (Ein) v += D.escale * Ein[first + i];
+          const int u0 = g0[i], u1 = g1[i];
+          if (u0 >= 0) v += W0[u0];
+          if (u1 >= 0) v += W1[u1];
+          vec[i] = (T)v;
+        }
+        for (int i = hi0 + tid; i < r1; i += kSolveThreads) {
+          double v = 0.0;
+          const int u0 = g0[i], u1 = g1[i];
+          if (u0 >= 0) v += W0[u0];
+          if (u1 >= 0) v += W1[u1];
+          vec[i] = (T)v;
+        }
+      }
+    } else {
+      const int32_t* ui = D.uidx + D.uoff[s];
+      for (int k = 0; k < nk; ++k) {
+        T* vec = vbuf + k * vcap;
+        const double* Yo = D.Y + (int64_t)o[k] * D.N;
+        const double* Xout = D.X + ((int64_t)o[k] * 9 + tau + 1) * D.N;
+        for (int i = r0 + tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
+        for (int u = tid; u < m; u += kSolveThreads) vec[n0pad + u] = (T)Xout[ui[u]];
+      }
+    }
+    __syncthreads();
+    // ---- pieces: wait, multiply, refill the buffer with the piece after next ----
+    const int64_t woff = D.woff[s];
+    int buf = 0;
+    bool ok_stage = true;
+    while (pa < r1) {
+      uint32_t& par = buf == 0 ? par0 : par1;
+      T* sb = stage + (int64_t)buf * half_elems;
+      if (!tc::mbar_wait(&bars[buf], par, kStageWait)) ok_stage = false;
+      par ^= 1u;
+      if (!__syncthreads_and(ok_stage ? 1 : 0)) {
+        if (tid == 0) raise_status(D.status, ORBIT_ERR_TIMEOUT);
+        ok_stage = false;
+        break;
+      }
+      const int64_t base = staged_prefix(kind, pa, n, ldn, ldm_st);
+      if (kind == 0) {
+        const int sq_end = min(pb, n);
+        const int64_t pb_off = pad4_prefix(sq_end) - pad4_prefix(min(pa, n));
+        const int pbase = max(pa, n);
+        auto partial = [&](auto g, int i, int gl, T(&acc)[K]) {
+          if (i < n)
+            dot_seg_smem<T, decltype(g)::value, K>(sb + (pad4_prefix(i) - base), vbuf, vcap, nk, 0, i, gl, acc);
+          else
+            dot_seg_smem<T, decltype(g)::value, K>(sb + pb_off + (int64_t)(i - pbase) * ldn, vbuf, vcap, nk, 0, n,
+                                                   gl, acc);
+        };
+        auto store = [&](int i, T(&acc)[K]) {
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (k < nk) {
+              const double y = (double)(vbuf[k * vcap + i] + acc[k]);
+              if (i < n) D.Y[(int64_t)o[k] * D.N + first + i] = y;
+              else D.W[(int64_t)o[k] * D.w_size + woff + (i - n)] = y;
+            }
+        };
+        const int Gl = group_lanes<T>(min(pb - 1, n));
+        ORBIT_GROUPED_ROWS_MULTI(T, K, Gl, pa, pb, warp, kWarps, partial, store);
+      } else {
+        const int64_t qr_off = (int64_t)(pb - pa) * ldn - (floor4_prefix(pb) - floor4_prefix(pa));
+        auto partial = [&](auto g, int i, int gl, T(&acc)[K]) {
+          constexpr int Gv = decltype(g)::value;
+          const int c0 = i & ~3;
+          const T* row = sb + ((int64_t)(i - pa) * ldn - (floor4_prefix(i) - floor4_prefix(pa)));
+          dot_seg_smem<T, Gv, K>(row, vbuf + c0, vcap, nk, i - c0, n - c0, gl, acc);
+          if (m > 0) dot_seg_smem<T, Gv, K>(sb + qr_off + (int64_t)(i - pa) * ldm, vbuf + n0pad, vcap, nk, 0, m, gl, acc);
+        };
+        auto store = [&](int i, T(&acc)[K]) {
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (k < nk) D.X[((int64_t)o[k] * 9 + tau + 1) * D.N + first + i] = (double)acc[k];
+        };
+        const int Gl = group_lanes<T>(n - pa + m);
+        ORBIT_GROUPED_ROWS_MULTI(T, K, Gl, pa, pb, warp, kWarps, partial, store);
+      }
+      __syncthreads();  // buffer `buf` consumed
+      pa = pb;
+      pb = pc;
+      if (pb < r1) {
+        pc = piece_end(kind, pb, r1, n, ldn, ldm_st, half_elems);
+        if (warp == 0) issue_piece<T>(SQ, kind, pb, pc, n, m, ldn, ldm_st, sb, &bars[buf], pol);
+      } else {
+        pc = pb;
+      }
+      buf ^= 1;
+    }
+    if (!ok_stage) break;
+    if (tid == 0) {
+      __threadfence();
       red_release_add(cbase + (tau * 2 + (kind == 0 ? 0 : 1)) * D.nsuper + s, 1);
     }
   }
@@ -781,6 +1261,26 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
     x[i] += escale * e[i];
 }
 
+// The staged chain kernel serves the non-transposed sweeps unless
+// ORBIT_B200_CHAIN_STAGED=0; ORBIT_B200_STAGE_KB sets each of its two stage
+// buffers (default 16 KB, at least one staged row).
+bool staged_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("ORBIT_B200_CHAIN_STAGED");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+int staged_half_bytes() {
+  static const int b = [] {
+    const char* e = std::getenv("ORBIT_B200_STAGE_KB");
+    const int kb = e ? std::atoi(e) : 16;
+    return std::min(std::max(kb, 4), 96) * 1024;
+  }();
+  return b;
+}
+
 template <typename T>
 int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, int trans, int tau0,
                    int tau1, const double* E, double escale, cudaStream_t st, bool never_ready = false) {
@@ -790,10 +1290,10 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.first = sy->d.first; D.n = sy->d.n; D.m = sy->d.m; D.parent = sy->d.parent;
   D.child = sy->d.child; D.uidx = sy->d.uidx; D.rel = sy->d.rel; D.ldn = sy->d.ldn; D.ldm = sy->d.ldm;
   D.ginv = sy->d.ginv; D.ginv_off = sy->d.ginv_off;
-  // Right-hand sides on one factor set go through the multi-RHS kernel in
-  // groups of K (non-transposed sweeps of row-chunk tasks).
+  // Right-hand sides on one factor set go through the multi-RHS kernels in
+  // groups of K (row-chunk tasks, forward and transposed sweeps).
   constexpr int KM = sizeof(T) == 4 ? 4 : 2;
-  const bool multi = !trans && !never_ready && f->n_sets == 1 && B >= 2 && S.max_sub_front == 0;
+  const bool multi = !never_ready && f->n_sets == 1 && B >= 2 && S.max_sub_front == 0;
   const int Bt = multi ? (B + KM - 1) / KM : B;  // task groups per (node chunk, bin)
   // schedule by batch size: small chunks shorten one orbit's critical path,
   // large ones cut per-task overhead when many orbits fill the GPU
@@ -836,9 +1336,48 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   int dev = 0, sms = 0, occ = 0;
   ORBIT_CUDA_TRY(cudaGetDevice(&dev));
   ORBIT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (!trans && !never_ready && S.max_sub_front == 0 && staged_enabled()) {
+    // factor rows staged in shared memory by bulk copies (k_chain_staged)
+    int maxrow = 4;
+    for (int s = 0; s < S.nsuper; ++s)
+      maxrow = std::max(maxrow, S.ldn[s] + (S.m[s] > 0 ? S.ldm[s] : 0));
+    int half = staged_half_bytes() / (int)sizeof(T);
+    half = (std::max(half, maxrow) + 3) & ~3;
+    const int vcap = (S.max_front + 8 + 3) & ~3;
+    const int K = multi ? KM : 1;
+    const size_t ssmem = sizeof(T) * ((size_t)2 * half + (size_t)K * vcap);
+    const void* fn = multi ? (const void*)k_chain_staged<T, KM> : (const void*)k_chain_staged<T, 1>;
+    {
+      int r0 = allow_max_smem(fn);
+      if (r0) return r0;
+    }
+    ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kSolveThreads, ssmem));
+    if (occ < 1) {
+      set_last_error("staged chain kernel cannot be resident (shared memory)");
+      return ORBIT_ERR_INTERNAL;
+    }
+    int grid = sms * occ;
+    if (grid > D.total) grid = D.total;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (f->prof_on) {
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0, st);
+    }
+    if (multi) k_chain_staged<T, KM><<<grid, kSolveThreads, ssmem, st>>>(D, vcap, half);
+    else k_chain_staged<T, 1><<<grid, kSolveThreads, ssmem, st>>>(D, vcap, half);
+    note_launch();
+    if (f->prof_on) {
+      cudaEventRecord(e1, st);
+      f->prof_chain.push_back({e0, e1});
+      f->prof_chain_bytes += (double)B * (tau1 - tau0) * S.fac_nnz * sizeof(T);
+    }
+    ORBIT_CUDA_TRY(cudaGetLastError());
+    return ORBIT_OK;
+  }
   if (multi) {
     const int vcap = (S.max_front + 8 + 3) & ~3;
-    const size_t msmem = sizeof(T) * (size_t)KM * vcap;
+    const size_t msmem = sizeof(T) * ((size_t)KM * vcap + (size_t)KM * kWarps * 32);
     {
       int r0 = allow_max_smem((const void*)k_chain_multi<T, KM>);
       if (r0) return r0;
@@ -864,6 +1403,12 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
       f->prof_chain_bytes += (double)B * (tau1 - tau0) * S.fac_nnz * sizeof(T);
     }
     ORBIT_CUDA_TRY(cudaGetLastError());
+    if (trans && E) {
+      dim3 g((unsigned)((S.N + 255) / 256), B);
+      k_add_forcing<<<g, 256, 0, st>>>(X, E, d_orbit_ids, S.N, tau0, escale);
+      note_launch();
+      ORBIT_CUDA_TRY(cudaGetLastError());
+    }
     return ORBIT_OK;
   }
   ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_chain<T>, kSolveThreads, smem));

@@ -46,14 +46,18 @@ class MetDevice:
             if name == "cmfmc" and (a.size == 0 or not np.any(a)):
                 continue
             self.t[name] = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
-        rho = met.rho().reshape(-1)
+        self.pressure_form = not bool(getattr(met, "concentration_state", True))
+        # state weights: rho in the concentration form, 1 in the pressure form
+        rho = met.state_weights().reshape(-1)
         self.rho = torch.as_tensor(rho, device=device)
         self.struct = _lib.MetT(**{k: _lib.ptr(self.t.get(k)) for k in _MET_FIELDS},
-                                dlat=self.dlat, dlon=self.dlon, split=int(self.split))
+                                dlat=self.dlat, dlon=self.dlon, split=int(self.split),
+                                pressure_form=int(self.pressure_form))
 
 
 def assemble_transport(met: MetDevice, with_rowsum: bool = False):
-    """K1: [7, N] concentration-form transport stencil (and pressure-form row sums)."""
+    """K1: [7, N] transport stencil (concentration form unless the grid is in
+    the pressure form) and, optionally, the pressure-form row sums."""
     T = torch.empty((7, met.N), dtype=torch.float64, device=met.rho.device)
     rs = torch.empty(met.N, dtype=torch.float64, device=met.rho.device) if with_rowsum else None
     _lib.check(_lib.lib().orbit_assemble_transport(met.nz, met.ny, met.nx, C.byref(met.struct),
@@ -76,6 +80,59 @@ def stencil_to_csr(T: np.ndarray, nz: int, ny: int, nx: int):
         rows.append(c[m]); cols.append(c[m] + off[d]); vals.append(T[d][m])
     return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                          shape=(N, N))
+
+
+SPECIES_FIELD_NAMES = ("Dz", "particle_dry_dep", "nh3_dry_dep", "so2_dry_dep", "nox_dry_dep", "hno3_dry_dep",
+                       "o3_dry_dep", "is_land", "voc_dry_dep", "particle_wet_dep", "other_gas_wet_dep",
+                       "so2_wet_dep", "nh_part", "no3_part", "fp_vbs", "fp_vbs_surface", "j_no2", "so2_ox",
+                       "nox_ox", "o3_loss", "co_loss", "archive_oh")
+N_SPECIES_ALL = 14
+# (target, source) of the rows of the coupling output, in order
+COUPLINGS = ((5, 3), (6, 4), (0, 12), (9, 0), (10, 9), (11, 10))
+
+
+def species_diagonals(nz: int, ny: int, nx: int, fields: dict, a_photo: float = 0.0, k_age: float = 0.0,
+                      aging_gain: float = 1.0, device="cuda"):
+    """K1b: (14, N) species sink diagonals and (6, N) source-coupling diagonals
+    of one bin from its per-cell fields (names as ``SPECIES_FIELD_NAMES``;
+    optional fields may be missing or None)."""
+    _require_cuda()
+    N = nz * ny * nx
+    keep = {}
+    kw = {}
+    for name in SPECIES_FIELD_NAMES:
+        a = fields.get(name)
+        if a is None:
+            kw[name] = 0
+            continue
+        t = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device) \
+            if not isinstance(a, torch.Tensor) else a.to(device=device, dtype=torch.float64).contiguous()
+        keep[name] = t
+        kw[name] = _lib.ptr(t)
+    st = _lib.SpeciesFieldsT(**kw, a_photo=float(a_photo), k_age=float(k_age), aging_gain=float(aging_gain))
+    d = torch.empty((N_SPECIES_ALL, N), dtype=torch.float64, device=device)
+    k = torch.empty((len(COUPLINGS), N), dtype=torch.float64, device=device)
+    _lib.check(_lib.lib().orbit_species_diagonals(nz, ny, nx, C.byref(st), _lib.ptr(d), _lib.ptr(k), _stream()))
+    return d, k
+
+
+def source_coupling(e: torch.Tensor, sources, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """out[tau] = e[tau] - sum over sources of kdiag[tau] * c[tau + shift] for one
+    target species; ``sources`` is a list of (kdiag (8, N), orbit (9, N), shift)."""
+    e = e.contiguous()
+    N = e.shape[-1]
+    out = e.clone() if out is None else out
+    if not sources:
+        if out.data_ptr() != e.data_ptr():
+            out.copy_(e)
+        return out
+    kd = torch.stack([s[0] for s in sources]).contiguous()
+    orbs = [s[1].contiguous() for s in sources]
+    cp = _lib.ptr_array([_lib.ptr(o) for o in orbs])
+    sh = (C.c_int * len(sources))(*[int(s[2]) for s in sources])
+    _lib.check(_lib.lib().orbit_source_coupling(N, len(sources), cp, sh, _lib.ptr(kd), _lib.ptr(e), _lib.ptr(out),
+                                                _stream()))
+    return out
 
 
 def fct_source(met: MetDevice, c: torch.Tensor, dt: float = DTAU, limited: bool = True):

@@ -72,7 +72,8 @@ def met_from_griddata(g) -> MetBin:
                   u_plus_e=u_plus_e, u_minus_e=np.maximum(-u_e, 0.0), v_n=v_n, v_plus_n=v_plus_n,
                   v_minus_n=np.maximum(-v_n, 0.0), kxxyy=_arr(g, "Kxxyy"), kzz=_arr(g, "Kzz"),
                   w_plus=w_plus, w_minus=w_minus, cmfmc=cm,
-                  kmu=_arr(g, "K_meander_u", zeros), kmv=_arr(g, "K_meander_v", zeros), split=split)
+                  kmu=_arr(g, "K_meander_u", zeros), kmv=_arr(g, "K_meander_v", zeros), split=split,
+                  concentration_state=bool(getattr(g, "concentration_state", True)))
 
 
 def griddata_like(m: MetBin, **extra) -> SimpleNamespace:
@@ -85,7 +86,7 @@ def griddata_like(m: MetBin, **extra) -> SimpleNamespace:
         U_minus_face_e=m.u_minus_e, V_face_n=m.v_n, V_plus_face_n=m.v_plus_n, V_minus_face_n=m.v_minus_n,
         Kzz=m.kzz, Kxxyy=m.kxxyy, K_meander_u=m.kmu, K_meander_v=m.kmv, omega_edge=w,
         omega_edge_plus=m.w_plus, omega_edge_minus=m.w_minus, has_interface_omega=True, CMFMC=m.cmfmc,
-        periodic_lon=False, concentration_state=True)
+        periodic_lon=False, concentration_state=bool(m.concentration_state))
     for k, v in extra.items():
         setattr(ns, k, v)
     return ns

@@ -149,6 +149,21 @@ def _emissions_for(emissions_SN, s, N):
     return [emissions_SN[t, s * N:(s + 1) * N] for t in range(N_BINS)]
 
 
+def _diag_of(K, N):
+    """The diagonal of a coupling block, which must be diagonal (every K block
+    of assemble_species_operators is, operator.py:419-547)."""
+    import scipy.sparse as sp
+    C = sp.coo_matrix(K)
+    if C.shape != (N, N):
+        raise ValueError(f"coupling block has shape {C.shape}, expected ({N}, {N})")
+    off = (C.row != C.col) & (C.data != 0)
+    if np.any(off):
+        raise ValueError("the device coupling takes diagonal K blocks only")
+    d = np.zeros(N)
+    np.add.at(d, C.row[C.row == C.col], C.data[C.row == C.col])
+    return d
+
+
 def solve_orbit_all_species(L_species_per_bin, K_sources_per_bin, emissions_SN, N, umfpack_sym=None,
                             perm=None, tol=1e-6, maxiter=200, verbose=True, c_warm_SN=None,
                             lu_cache=None, skip_solve_species=None, cached_orbits=None,
@@ -160,8 +175,13 @@ def solve_orbit_all_species(L_species_per_bin, K_sources_per_bin, emissions_SN, 
     Arguments and result as in the reference (orbit.py:468-559).  ``umfpack_sym``
     may be omitted: the symbolic is then built from the first operator's
     pattern.  ``precision=32`` selects FP32 factors with FP64 refinement.
+    Solved orbits stay on the device between waves: the coupled right-hand
+    sides e_tau - K c_src[tau] (or c_src[tau + 1] for ``endbin_keys``,
+    orbit.py:249-307) are formed there (``orbit_source_coupling``); the host
+    receives the orbits once, at the end.
     """
     import torch
+    from . import device
     from .device import FactorBatch
 
     n_species = len(L_species_per_bin[0])
@@ -170,13 +190,14 @@ def solve_orbit_all_species(L_species_per_bin, K_sources_per_bin, emissions_SN, 
         first = next(L for L in L_species_per_bin[0] if L is not None)
         umfpack_sym = umfpack_symbolic(first, verbose=verbose)
     sym = umfpack_sym.sym if isinstance(umfpack_sym, DeviceSymbolic) else umfpack_sym
-    orbits = {}
+    dev_orbits = {}  # species -> (9, N) device tensor
+    host_orbits = {}  # species -> list of host arrays (seeds and cached copies, returned as given)
     gmres_iters = np.zeros(n_species, dtype=int)
     gmres_resid = np.zeros(n_species)
     periodicity = np.zeros(n_species)
     if seed_orbits is not None:
         for s, orb in seed_orbits.items():
-            orbits[s] = [c.copy() for c in orb]
+            host_orbits[s] = [np.array(c, dtype=np.float64, copy=True) for c in orb]
     skip = set(skip_solve_species or ())
     sources_for_target = {}
     for (tgt, src) in K_sources_per_bin[0].keys():
@@ -184,39 +205,59 @@ def solve_orbit_all_species(L_species_per_bin, K_sources_per_bin, emissions_SN, 
     order = [s for s in _SOLVE_ORDER if s < n_species] + [s for s in range(n_species) if s >= len(_SOLVE_ORDER)]
     waves = _build_solve_waves(sources_for_target, order, skip)
     fresh_cache = {}
+    kdiag_cache = {}
 
     def log(msg):
         if verbose:
             print(msg, flush=True)
 
+    def name(s):
+        return _SPECIES_NAMES[s] if s < len(_SPECIES_NAMES) else s
+
+    def orbit_dev(s, snap_dev, snap_host):
+        if s in snap_dev:
+            return snap_dev[s]
+        if s in snap_host:
+            return torch.as_tensor(np.stack(snap_host[s]), device="cuda")
+        raise KeyError(f"orbits[{s}] missing for a target; seed orbits are needed for cyclic source DAGs")
+
+    def kdiag(tgt, src):
+        key = (tgt, src)
+        if key not in kdiag_cache:
+            kdiag_cache[key] = torch.as_tensor(
+                np.stack([_diag_of(K_sources_per_bin[t][key], N) for t in range(N_BINS)]), device="cuda")
+        return kdiag_cache[key]
+
     for wave in waves:
-        snap = dict(orbits)
-        todo = []  # (s, e_list, warm)
+        snap_dev, snap_host = dict(dev_orbits), dict(host_orbits)
+        todo = []  # (s, E (8, N) device, warm)
         for s in wave:
             if s in skip and cached_orbits is not None and s in cached_orbits:
-                orbits[s] = [c.copy() for c in cached_orbits[s]]
-                log(f"  [{_SPECIES_NAMES[s] if s < len(_SPECIES_NAMES) else s}]\n"
-                    f"    [cache] skipped factor + solve (operator+RHS unchanged)")
+                host_orbits[s] = [np.array(c, copy=True) for c in cached_orbits[s]]
+                dev_orbits.pop(s, None)
+                log(f"  [{name(s)}]\n    [cache] skipped factor + solve (operator+RHS unchanged)")
                 continue
-            e_list = [e.copy() for e in _emissions_for(emissions_SN, s, N)]
+            e_host = np.stack([np.asarray(x, dtype=np.float64) for x in _emissions_for(emissions_SN, s, N)])
+            if extra_rhs_per_bin_per_species is not None and s in extra_rhs_per_bin_per_species:
+                e_host = e_host + np.stack([np.asarray(x, dtype=np.float64)
+                                            for x in extra_rhs_per_bin_per_species[s]])
+            E = torch.as_tensor(np.ascontiguousarray(e_host), device="cuda")
+            srcs = []
             for src in sources_for_target.get(s, []):
-                if src not in snap:
+                if src not in snap_dev and src not in snap_host:
                     raise KeyError(f"orbits[{src}] missing for target s={s}; seed orbits are needed "
                                    "for cyclic source DAGs")
-                for t in range(N_BINS):
-                    K = K_sources_per_bin[t][(s, src)]
-                    c_src = snap[src][t + 1] if (endbin_keys is not None and (s, src) in endbin_keys) \
-                        else snap[src][t]
-                    e_list[t] = e_list[t] - K @ c_src
-            if extra_rhs_per_bin_per_species is not None and s in extra_rhs_per_bin_per_species:
-                e_list = [e_list[t] + extra_rhs_per_bin_per_species[s][t] for t in range(N_BINS)]
-            if all(not np.any(e) for e in e_list):
-                orbits[s] = [np.zeros(N) for _ in range(N_BINS + 1)]
-                log(f"  [{_SPECIES_NAMES[s] if s < len(_SPECIES_NAMES) else s}]\n"
-                    "    [zero-source] skipped factor + solve (RHS identically zero)")
+                shift = 1 if (endbin_keys is not None and (s, src) in endbin_keys) else 0
+                srcs.append((kdiag(s, src), orbit_dev(src, snap_dev, snap_host), shift))
+            if srcs:
+                device.source_coupling(E, srcs, out=E)
+            if not bool((E != 0).any()):
+                dev_orbits[s] = torch.zeros((N_BINS + 1, N), dtype=torch.float64, device="cuda")
+                host_orbits.pop(s, None)
+                log(f"  [{name(s)}]\n    [zero-source] skipped factor + solve (RHS identically zero)")
                 continue
             warm = None if c_warm_SN is None else np.asarray(c_warm_SN[s * N:(s + 1) * N], dtype=np.float64)
-            todo.append((s, e_list, warm))
+            todo.append((s, E, warm))
         if not todo:
             continue
         # group: species with cached factors solve in their cached batch, the rest in a new one
@@ -248,28 +289,33 @@ def solve_orbit_all_species(L_species_per_bin, K_sources_per_bin, emissions_SN, 
             if nm != fb.n_orbits or any(q != k for k, (_, q) in enumerate(members)):
                 # solve slots 0..nm-1 mapped onto the members' factor sets
                 slot_fb = _remap(fb, [q for (_, q) in members])
-            E = torch.as_tensor(np.stack([np.stack(it[1]) for it, _ in members]), device="cuda")
+            E = torch.stack([it[1] for it, _ in members])
             warm = None
             if any(it[2] is not None for it, _ in members):
                 warm = torch.as_tensor(np.stack([it[2] if it[2] is not None else np.zeros(N)
                                                  for it, _ in members]), device="cuda")
-            orb, info = slot_fb.solve(E, c_warm=warm if warm is not None else None, tol=tol, maxiter=maxiter)
-            orb = orb.cpu().numpy()
+            orb, info = slot_fb.solve(E, c_warm=warm, tol=tol, maxiter=maxiter)
             for k, (it, q) in enumerate(members):
                 s = it[0]
-                orbits[s] = [orb[k, t].copy() for t in range(N_BINS + 1)]
+                dev_orbits[s] = orb[k]
+                host_orbits.pop(s, None)
                 gmres_iters[s] = int(info[k, 0])
                 gmres_resid[s] = float(info[k, 1])
                 periodicity[s] = float(info[k, 2])
                 fresh_cache[s] = SpeciesFactors(fb, q)
-                neg = int(np.sum(orb[k] < 0))
-                log(f"  [{_SPECIES_NAMES[s] if s < len(_SPECIES_NAMES) else s}]\n"
-                    f"    GMRES: {int(info[k, 0])} iter ({time.time() - t1:.2f}s batch of {nm}), "
-                    f"resid={info[k, 1]:.1e}, period={info[k, 2]:.1e}, neg={neg}/{orb[k].size}")
+                if verbose:
+                    neg = int((orb[k] < 0).sum())
+                    log(f"  [{name(s)}]\n"
+                        f"    GMRES: {int(info[k, 0])} iter ({time.time() - t1:.2f}s batch of {nm}), "
+                        f"resid={info[k, 1]:.1e}, period={info[k, 2]:.1e}, neg={neg}/{orb[k].numel()}")
                 if keep_lu_species is not None and s not in keep_lu_species:
                     fresh_cache.pop(s, None)
                 for t in range(N_BINS):
                     L_species_per_bin[t][s] = None
+    orbits = dict(host_orbits)
+    for s, o in dev_orbits.items():
+        oh = o.cpu().numpy()
+        orbits[s] = [oh[t].copy() for t in range(N_BINS + 1)]
     result = {"orbits": orbits, "gmres_iters": gmres_iters, "gmres_resid": gmres_resid,
               "periodicity": periodicity}
     if return_lu_cache:

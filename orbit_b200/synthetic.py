@@ -80,6 +80,7 @@ class MetBin:
     kmu: np.ndarray
     kmv: np.ndarray
     split: bool = True
+    concentration_state: bool = True  # GridData.concentration_state (grid_data.py:71)
 
     @property
     def N(self) -> int:
@@ -97,6 +98,14 @@ class MetBin:
         """dP / (g Dz), 1 where a cell is degenerate (``grid_data.py:543-554``)."""
         ok = (self.dP > 0) & (self.Dz > 0)
         return np.where(ok, self.dP / (GRAVITY * np.where(ok, self.Dz, 1.0)), 1.0)
+
+    def state_weights(self) -> np.ndarray:
+        """Weights of the transported state: rho in the concentration form, 1 in
+        the pressure form (``_state_weights``, ``orbit/core/fct.py:451-456``;
+        ``mass_balance_diagnostics``, ``orbit/core/operator.py:626``)."""
+        if self.concentration_state:
+            return self.rho()
+        return np.ones((self.nz, self.ny, self.nx))
 
 
 @dataclass

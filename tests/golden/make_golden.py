@@ -3,7 +3,10 @@
 Run in a container where the reference checkout is importable (its default
 location is used unless ORBIT_REFERENCE is set):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                   # every golden file
+    python tests/golden/make_golden.py --pressure-form   # only pressure_form.npz
+    python tests/golden/make_golden.py --species         # only species_ops.npz
+    python tests/golden/make_golden.py --closure         # only closure.npz
 
 It builds reference ``GridData`` objects from this repository's seeded
 synthetic meteorology (``orbit_b200.synthetic``), calls the reference's own
@@ -38,6 +41,7 @@ from orbit_b200 import synthetic  # noqa: E402
 
 def to_griddata(m: synthetic.MetBin, vd=None, wet=None) -> GridData:
     g = GridData()
+    g.concentration_state = bool(m.concentration_state)
     g.nz, g.ny, g.nx = m.nz, m.ny, m.nx
     g.lat, g.lon, g.dlat, g.dlon = m.lat.copy(), m.lon.copy(), m.dlat, m.dlon
     g.dP, g.Dz = m.dP.copy(), m.Dz.copy()
@@ -167,5 +171,181 @@ def main():
           "adj iters", ainfo["gmres_iters"])
 
 
+def pressure_form():
+    """Goldens of a grid in the pressure form (GridData.concentration_state
+    False): the reference then keeps the assembled block as it is
+    (operator.py:341), weights the FCT state and the mass-balance rows by 1
+    (fct.py:451-456, operator.py:626)."""
+    rng = np.random.default_rng(23)
+    nz, ny, nx = 4, 7, 8
+    m = synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=2000.0, rho_profile=True,
+                               cmfmc_frac=0.3, wind_std=6.0)
+    m.concentration_state = False
+    idx = CellIndexer(nz, ny, nx)
+    g = to_griddata(m)
+    out = met_arrays("pf_", m)
+    out.update(csc_arrays("pf_T_", operator.assemble_transport_block(g, idx)))
+    kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    c = ((1.0 + np.sin(0.8 * ii) * np.cos(0.6 * jj) + 0.2 * kk + rng.random((nz, ny, nx))) * 1e-9).reshape(-1)
+    out["pf_c"] = c
+    out["pf_fct_d"] = fct.compute_horizontal_fct_source(g, idx, c, DTAU)
+    out["pf_fct_d_unlim"] = fct.compute_horizontal_fct_source(g, idx, c, DTAU, limited=False)
+    out.update(csc_arrays("pf_fct_L_", fct.assemble_fct_linear_operator(g, idx, c, DTAU)))
+    mb = operator.mass_balance_diagnostics([g], idx)
+    keys = ["interior_median", "interior_p90", "interior_p99", "interior_max", "top_median", "top_p90"]
+    out["pf_mb_keys"] = np.array(keys)
+    out["pf_mb_vals"] = np.array([mb[k] for k in keys])
+    path = os.path.join(HERE, "pressure_form.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+SPECIES_FIELDS = ("particle_dry_dep", "NH3_dry_dep", "SO2_dry_dep", "NOx_dry_dep", "HNO3_dry_dep", "O3_dry_dep",
+                  "VOC_dry_dep", "particle_wet_dep", "other_gas_wet_dep", "SO2_wet_dep", "NHPartitioning",
+                  "NHPartitioningEq", "NO3Partitioning", "NO3PartitioningEq", "SO2oxidation", "archive_OH",
+                  "j_no2_soa", "is_land", "F_p_vbs", "F_p_vbs_surface")
+
+
+def species_operators():
+    """Goldens of assemble_species_operators (operator.py:371-595) on two grids:
+    'full' carries every optional field (HNO3/O3/VOC dry deposition, land
+    mask, both partition fractions, VBS particle fractions, j(NO2) with the
+    photolytic sink on, archive OH for the aging cascade, NOx/O3/CO rates);
+    'min' only the required ones (fallback velocities, zero NO3 fraction,
+    pure-particle VBS, no aging, SO2 rate by override)."""
+    rng = np.random.default_rng(41)
+    nz, ny, nx = 4, 6, 7
+    idx = CellIndexer(nz, ny, nx)
+    N = idx.N
+    m = synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=1000.0, rho_profile=True, cmfmc_frac=0.3)
+    out = met_arrays("sp_", m)
+
+    def u(lo, hi, shape):
+        return rng.uniform(lo, hi, shape)
+
+    full = {"particle_dry_dep": u(1e-4, 5e-3, (nz, ny, nx)), "NH3_dry_dep": u(1e-3, 2e-2, (nz, ny, nx)),
+            "SO2_dry_dep": u(1e-3, 1e-2, (nz, ny, nx)), "NOx_dry_dep": u(1e-4, 3e-3, (nz, ny, nx)),
+            "HNO3_dry_dep": u(1e-2, 5e-2, (nz, ny, nx)), "O3_dry_dep": u(5e-4, 8e-3, (nz, ny, nx)),
+            "VOC_dry_dep": u(5e-4, 3e-3, (nz, ny, nx)), "particle_wet_dep": u(0, 2e-5, (nz, ny, nx)),
+            "other_gas_wet_dep": u(0, 5e-5, (nz, ny, nx)), "SO2_wet_dep": u(0, 3e-5, (nz, ny, nx)),
+            "NHPartitioning": u(0, 1, (nz, ny, nx)), "NHPartitioningEq": u(0, 1, (nz, ny, nx)),
+            "NO3Partitioning": u(0, 1, (nz, ny, nx)), "NO3PartitioningEq": u(0, 1, (nz, ny, nx)),
+            "SO2oxidation": u(1e-7, 1e-5, (nz, ny, nx)), "archive_OH": u(1e5, 5e6, (nz, ny, nx)),
+            "j_no2_soa": u(0, 8e-3, (nz, ny, nx)), "is_land": (rng.random((ny, nx)) > 0.3).astype(np.float64),
+            "F_p_vbs": u(-0.1, 1.1, (5, nz, ny, nx)), "F_p_vbs_surface": u(0, 1, (5, ny, nx))}
+    rates = {"nox_to_no3_rate": u(1e-7, 1e-5, (nz, ny, nx)), "o3_loss_rate": u(1e-7, 1e-5, (nz, ny, nx)),
+             "co_loss_rate": u(1e-8, 1e-6, (nz, ny, nx))}
+    minimal = {k: full[k] for k in ("particle_dry_dep", "NH3_dry_dep", "SO2_dry_dep", "NOx_dry_dep",
+                                    "particle_wet_dep", "other_gas_wet_dep", "SO2_wet_dep", "NHPartitioning")}
+    so2_override = u(1e-7, 1e-5, (nz, ny, nx))
+    for k, v in full.items():
+        out[f"full_{k}"] = v
+    for k, v in rates.items():
+        out[f"rate_{k}"] = v
+    out["so2_override"] = so2_override
+    os.environ["ORBIT_VBS_A_PHOTO"] = "4.0e-4"
+    for tag, fields, kw in (("full", full, rates), ("min", minimal, {"so2_ox_rate": so2_override})):
+        g = to_griddata(m)
+        for k, v in fields.items():
+            setattr(g, k, v.copy())
+        for part in ("marginal", "equilibrium"):
+            res = operator.assemble_species_operators(g, idx, verbose=False, return_D_per_species=True,
+                                                      partitioning=part, **kw)
+            L, K, T, d, D, Kage = res
+            key = f"{tag}_{part}"
+            out[f"{key}_d"] = d
+            out[f"{key}_D"] = np.stack([np.asarray(x.diagonal()) for x in D])
+            out[f"{key}_Kkeys"] = np.array(sorted(K.keys()), dtype=np.int64).reshape(-1, 2)
+            out[f"{key}_Kdiag"] = np.stack([np.asarray(K[k].diagonal()) for k in sorted(K.keys())])
+            out[f"{key}_Kagekeys"] = np.array(sorted(Kage.keys()), dtype=np.int64)
+            out[f"{key}_Kage"] = (np.stack([np.asarray(Kage[k].diagonal()) for k in sorted(Kage.keys())])
+                                  if Kage else np.zeros((0, N)))
+            L1 = L[1].tocsc()
+            L1.sum_duplicates()
+            L1.sort_indices()
+            out.update(csc_arrays(f"{key}_L1_", L1))
+            out.update(csc_arrays(f"{key}_T_", T))
+    del os.environ["ORBIT_VBS_A_PHOTO"]
+    path = os.path.join(HERE, "species_ops.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def closure():
+    """Goldens of the closure loop's pieces: IsorropiaLUT.query
+    (isorropia_lut.py:116-147) on a small synthetic 7-D table written in the
+    reference's file layout (points inside, on grid nodes and outside the
+    axes, where the reference extrapolates), and an AndersonAccelerator
+    (closure_iteration.py:568-694) sequence with the safeguard on a linear
+    fixed-point map."""
+    import tempfile
+    from orbit.core.isorropia_lut import IsorropiaLUT
+    from orbit.core.closure_iteration import AndersonAccelerator
+    rng = np.random.default_rng(57)
+    axes = {"so4_axis": np.array([0.0, 1.0, 4.0, 10.0]), "nh_axis": np.array([0.0, 2.0, 8.0]),
+            "no3_axis": np.array([0.0, 3.0, 9.0]), "ca_axis": np.array([0.0, 0.5]),
+            "na_axis": np.array([0.0, 0.3]), "t_axis": np.array([260.0, 280.0, 300.0]),
+            "rh_axis": np.array([0.1, 0.4, 0.7, 0.95])}
+    shape = tuple(len(a) for a in axes.values())
+    fields = {"f_nh4": rng.uniform(-0.1, 1.1, shape).astype(np.float32),
+              "f_no3": rng.uniform(-0.1, 1.1, shape).astype(np.float32),
+              "aerosol_water": rng.uniform(-1.0, 50.0, shape).astype(np.float32),
+              "ph": rng.uniform(1.0, 6.0, shape).astype(np.float32)}
+    out = {f"lut_{k}": v for k, v in {**axes, **fields}.items()}
+    lo = np.array([a[0] for a in axes.values()])
+    hi = np.array([a[-1] for a in axes.values()])
+    pts = lo + (hi - lo) * rng.uniform(-0.15, 1.15, (400, 7))
+    nodes = np.stack([rng.choice(a, 50) for a in axes.values()], axis=1)
+    pts = np.concatenate([pts, nodes])
+    out["lut_pts"] = pts
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "lut.npz")
+        np.savez(path, **axes, **fields)
+        os.environ["ORBIT_LUT_CACHE_DIR"] = os.path.join(tmp, "cache")
+        lut = IsorropiaLUT(path, fields=("f_nh4", "f_no3", "aerosol_water", "ph"))
+        res = lut.query(*[pts[:, d] for d in range(7)])
+        lut2 = IsorropiaLUT(path)
+        res2 = lut2.query(*[pts[:, d] for d in range(7)])
+        del os.environ["ORBIT_LUT_CACHE_DIR"]
+    out["lut_out"] = np.stack(res)
+    out["lut_out_two_fields"] = np.stack(res2)
+    # Anderson on g(x) = A x + b with A of spectral radius 0.9
+    n = 40
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = Q @ np.diag(rng.uniform(-0.9, 0.9, n)) @ Q.T
+    b = rng.standard_normal(n)
+    out["and_A"], out["and_b"] = A, b
+    for tag, kw in (("m3", dict(m=3, beta=1.0)), ("m2d", dict(m=2, beta=0.6, safeguard_factor=1.05))):
+        acc = AndersonAccelerator(**kw)
+        x = np.zeros(n)
+        xs, flags = [x.copy()], []
+        for _ in range(10):
+            x, ok = acc.apply_with_safeguard(x, A @ x + b)
+            xs.append(x.copy())
+            flags.append(ok)
+        out[f"and_{tag}_x"] = np.stack(xs)
+        out[f"and_{tag}_ok"] = np.array(flags)
+        acc2 = AndersonAccelerator(**{k: v for k, v in kw.items() if k != "safeguard_factor"})
+        x = np.zeros(n)
+        xs = [x.copy()]
+        for _ in range(10):
+            x = acc2.update(x, A @ x + b)
+            xs.append(x.copy())
+        out[f"and_{tag}_x_unguarded"] = np.stack(xs)
+    path = os.path.join(HERE, "closure.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    main()
+    if "--pressure-form" in sys.argv:
+        pressure_form()
+    elif "--species" in sys.argv:
+        species_operators()
+    elif "--closure" in sys.argv:
+        closure()
+    else:
+        main()
+        pressure_form()
+        species_operators()
+        closure()

@@ -12,8 +12,19 @@ _NAMES = ("dP", "Dz", "u", "v", "u_plus", "u_minus", "v_plus", "v_minus", "u_e",
           "w_plus", "w_minus", "cmfmc", "kmu", "kmv", "lat", "lon")
 
 
+PRESSURE_FORM = os.path.join(os.path.dirname(GOLDEN), "pressure_form.npz")
+
+
 def load():
     return dict(np.load(GOLDEN))
+
+
+def load_pressure_form():
+    """Goldens of a grid in the pressure form (concentration_state False) and its MetBin."""
+    z = dict(np.load(PRESSURE_FORM))
+    m = met_bin(z, "pf_")
+    m.concentration_state = False
+    return z, m
 
 
 def met_bin(z, prefix):

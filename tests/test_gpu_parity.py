@@ -200,3 +200,24 @@ def test_config0_against_oracle():
     fb32.numeric(T, sinks)
     orb32, _ = fb32.solve(torch.as_tensor(sp0.emis, device="cuda")[None], tol=1e-8)
     assert _rel(orb32.cpu().numpy()[0], np.stack(ref)) < 1e-6
+
+
+def test_pressure_form_grid_matches_reference():
+    """A grid with concentration_state False through the drop-in modules: the
+    block as assembled, unit state weights in the FCT source, L_AD and the
+    mass-balance rows, against the reference's own outputs (golden)."""
+    from orbit_b200 import fct as dfct, operator as dop
+    from orbit_b200.grid import griddata_like
+    zp, m = golden_io.load_pressure_form()
+    g = griddata_like(m)
+    assert g.concentration_state is False
+    T = dop.assemble_transport_block(g)
+    assert _rel(T.toarray(), golden_io.csc(zp, "pf_T_").toarray()) < 1e-12
+    c = zp["pf_c"]
+    assert _rel(dfct.compute_horizontal_fct_source(g, None, c, 10800.0), zp["pf_fct_d"]) < 1e-12
+    assert _rel(dfct.compute_horizontal_fct_source(g, None, c, 10800.0, limited=False), zp["pf_fct_d_unlim"]) < 1e-12
+    L = dfct.assemble_fct_linear_operator(g, None, c, 10800.0)
+    assert _rel(L.toarray(), golden_io.csc(zp, "pf_fct_L_").toarray()) < 1e-12
+    mb = dop.mass_balance_diagnostics([g])
+    got = np.array([mb[str(k)] for k in zp["pf_mb_keys"]])
+    np.testing.assert_allclose(got, zp["pf_mb_vals"], rtol=1e-9, atol=1e-12)

@@ -96,3 +96,20 @@ def test_adjoint_solve():
     err = np.abs(np.stack(adj) - ref).max() / np.abs(ref).max()
     assert err < 1e-10
     assert info["periodicity"] < 1e-8
+
+
+def test_pressure_form_grid():
+    """concentration_state False: no similarity transform, unit state weights
+    in the FCT source, L_AD and the mass-balance rows (operator.py:341,
+    fct.py:451-456, operator.py:626)."""
+    zp, g = golden_io.load_pressure_form()
+    assert _close(assembly.transport_block(g), golden_io.csc(zp, "pf_T_"))
+    c = zp["pf_c"]
+    np.testing.assert_allclose(fct.fct_source(g, c, 10800.0), zp["pf_fct_d"], rtol=1e-12,
+                               atol=1e-12 * np.abs(zp["pf_fct_d"]).max())
+    np.testing.assert_allclose(fct.fct_source(g, c, 10800.0, limited=False), zp["pf_fct_d_unlim"],
+                               rtol=1e-12, atol=1e-12 * np.abs(zp["pf_fct_d_unlim"]).max())
+    assert _close(fct.fct_linear_operator(g, c, 10800.0), golden_io.csc(zp, "pf_fct_L_"))
+    mb = assembly.mass_balance_diagnostics([g])
+    got = np.array([mb[str(k)] for k in zp["pf_mb_keys"]])
+    np.testing.assert_allclose(got, zp["pf_mb_vals"], rtol=1e-9, atol=1e-12)

@@ -4,7 +4,8 @@ orbit_fct_source_noalloc serves callers that cannot allocate device memory
 where they apply the FCT correction (a host model that owns its whole device
 budget through its own pool, or a time loop that must not stall on the
 synchronization a cudaFree can cause); its scratch is a static device array
-shared by all calls.  Two calls in a row, with different inputs, must each
+shared by all calls.  Calls in a row, with different inputs (limited and
+unlimited), must each
 match orbit_fct_source called through the same C ABI, to the 1e-12 relative
 tolerance of the FCT parity tests; the second call also shows that nothing
 left in the shared scratch by the first leaks into it.  This file is named to
@@ -36,6 +37,7 @@ def test_noalloc_fct_matches_allocating_entry_point():
     inputs = [
         (met[0], torch.stack([c0, 2.0 * c0]), 1),          # limited, two vectors
         (met[1], torch.stack([c0.flip(0), c0 * 0.5]), 1),  # another bin, new data
+        (met[2], torch.stack([c0 * 3.0, c0.flip(0)]), 0),  # unlimited: no R+/R- pass
     ]
     for g, c, limited in inputs:
         md = device.MetDevice(g)
