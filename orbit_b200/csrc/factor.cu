@@ -1253,6 +1253,148 @@ __global__ void __launch_bounds__(128, 3) k_gemm_tc(FactorDev D, float* fronts, 
   if (warp == 1) tc::tmem_dealloc(tmem, 128);
 }
 
+// Trailing update of the blocked pivot LU on the tensor cores (fp32 fronts):
+// the 128 x 128 tile (tr, tc) beyond the pivot block [p0, q0) gets
+// C -= L[:, p0:q0] U[p0:q0, :] (K = nb <= 64) with split tf32 operands, the
+// part inside F22 (rows and columns >= n) left to the Schur pass, as k_update2
+// does on the CUDA cores.  All 128 threads load their operand rows (A: one
+// tile row each, 16-byte loads along K; B: one tile column each, coalesced
+// across the warp), split them into tf32 hi/lo and store them in the 64-byte
+// swizzled layout the MMA descriptors read; two k-blocks of 16 per round,
+// then one thread issues the MMAs into the tensor-memory accumulator.  Three
+// CTAs per SM overlap one tile's loads and epilogue with the others' MMAs.
+// Every wait is bounded; on a timeout the CTA leaves the tile untouched,
+// raises ORBIT_ERR_TIMEOUT and frees its tensor memory.
+constexpr int kUpdKb = 2;                                        // k-blocks of 16 per round
+constexpr size_t kUpdSmem = (size_t)kUpdKb * kTcStageBytes + 512;
+
+__global__ void __launch_bounds__(128, 3) k_update_tc(FactorDev D, float* fronts, int64_t i0, int p0,
+                                                      int* status) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t full, done;
+  __shared__ uint32_t tmem_base;
+  const uint32_t raw = tc::smem_u32(smem_raw);
+  unsigned char* sbuf = smem_raw + ((512u - (raw & 511u)) & 511u);
+  const int4 it = D.items[i0 + blockIdx.x];
+  const int s = it.x, tr = it.y, tcl = it.z;
+  const int n = D.n[s], m = D.m[s], ldf = D.ldf[s];
+  const int nb = min(64, n - p0);
+  const int q0 = p0 + nb;
+  const int r0 = q0 + 128 * tr, c0 = q0 + 128 * tcl;
+  const int lim = tc_node(D, n, m) ? n : n + m;
+  if (r0 >= lim || c0 >= lim) return;  // uniform over the CTA
+  const int M = min(128, lim - r0), N = min(128, lim - c0);
+  float* F = fronts + (int64_t)blockIdx.y * D.front_buf + D.front_off[s];
+  const float* A = F + (int64_t)r0 * ldf + p0;  // M x nb, row-major
+  const float* B = F + (int64_t)p0 * ldf + c0;  // nb x N, row-major
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, t = threadIdx.x;
+  if (t == 0) {
+    tc::mbar_init(&full, 128);
+    tc::mbar_init(&done, 1);
+    tc::fence_barrier_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&tmem_base, 128);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_tf32(128, 128);
+  const int nkb = (nb + tc::kCols - 1) / tc::kCols;
+  bool ok = true;
+  uint32_t ph = 0;
+  for (int kb0 = 0; kb0 < nkb && ok; kb0 += kUpdKb) {
+    const int nr = min(kUpdKb, nkb - kb0);
+    for (int h = 0; h < nr; ++h) {
+      float* At = reinterpret_cast<float*>(sbuf + h * kTcStageBytes);
+      float* Bt = At + 2 * tc::kTileFloats;
+      const int k0 = (kb0 + h) * tc::kCols;
+      // A row t: 16 values along K, 16-byte loads (rows start 16-byte aligned
+      // and p0, k0 are multiples of 16; a load that starts below nb stays inside
+      // the padded row); entries at k >= nb belong to the next pivot columns
+      // and are zeroed
+      float a[16];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (t < M && k0 + 4 * q < nb) v = *reinterpret_cast<const float4*>(A + (int64_t)t * ldf + k0 + 4 * q);
+        const int kq = k0 + 4 * q;
+        a[4 * q] = kq < nb ? v.x : 0.f;
+        a[4 * q + 1] = kq + 1 < nb ? v.y : 0.f;
+        a[4 * q + 2] = kq + 2 < nb ? v.z : 0.f;
+        a[4 * q + 3] = kq + 3 < nb ? v.w : 0.f;
+      }
+      // B column t: 16 values down K (consecutive t read consecutive columns)
+      float b[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) b[k] = (t < N && k0 + k < nb) ? B[(int64_t)(k0 + k) * ldf + t] : 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        store_split4(At, tc::swz(t, 4 * q), a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
+        store_split4(Bt, tc::swz(t, 4 * q), b[4 * q], b[4 * q + 1], b[4 * q + 2], b[4 * q + 3]);
+      }
+    }
+    tc::fence_proxy_async();
+    tc::mbar_arrive(&full);
+    if (t == 32) {
+      if (tc::mbar_wait(&full, ph, kTcWaitLimit)) {
+        tc::fence_after_sync();
+        for (int h = 0; h < nr; ++h) {
+          const uint32_t a0 = tc::smem_u32(sbuf + h * kTcStageBytes);
+          const uint32_t ahi = a0, alo = a0 + tc::kTileBytes, bhi = a0 + 2 * tc::kTileBytes,
+                         blo = a0 + 3 * tc::kTileBytes;
+#pragma unroll
+          for (int kk = 0; kk < tc::kCols / 8; ++kk) {
+            const uint32_t o = kk * 32;
+            tc::mma_tf32(tmem, tc::sw64_desc(ahi + o), tc::sw64_desc(bhi + o), idesc, ((kb0 + h) | kk) != 0);
+            tc::mma_tf32(tmem, tc::sw64_desc(ahi + o), tc::sw64_desc(blo + o), idesc, 1);
+            tc::mma_tf32(tmem, tc::sw64_desc(alo + o), tc::sw64_desc(bhi + o), idesc, 1);
+          }
+        }
+      }
+      tc::mma_commit(&done);
+    }
+    // the round's MMAs have read the operands before the buffers are refilled
+    if (!tc::mbar_wait(&done, ph, kTcWaitLimit)) ok = false;
+    ph ^= 1u;
+    tc::fence_after_sync();
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
+  }
+  if (ok) {
+    // each warp stages its 32 x 32 accumulator blocks through shared memory
+    // so that the update goes row by row, coalesced
+    float* sw = reinterpret_cast<float*>(sbuf) + warp * 32 * 33;
+    const int rows = min(32, M - warp * 32);
+    for (int cc = 0; cc < 4 && cc * 32 < N; ++cc) {
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) sw[lane * 33 + j] = v[j];
+      __syncwarp();
+      const int col = cc * 32 + lane;
+      if (col < N) {
+        float* C = F + (int64_t)(r0 + warp * 32) * ldf + c0 + col;
+        const bool f22_col = c0 + col >= n;
+        float c[32];
+#pragma unroll
+        for (int u = 0; u < 32; ++u)
+          if (u < rows) c[u] = C[(int64_t)u * ldf];
+#pragma unroll
+        for (int u = 0; u < 32; ++u)
+          if (u < rows && !(f22_col && r0 + warp * 32 + u >= n)) C[(int64_t)u * ldf] = c[u] - sw[u * 33 + lane];
+      }
+      __syncwarp();
+    }
+  } else if (t == 0) {
+    raise_status(status, ORBIT_ERR_TIMEOUT);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 1) tc::tmem_dealloc(tmem, 128);
+}
+
 inline int clamp_grid(int64_t blocks) {
   if (blocks < 1) return 1;
   if (blocks > (1 << 20)) return 1 << 20;
@@ -1283,7 +1425,7 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
   const size_t sm_diag = (3 * kNB * (kNB + 4) + 512) * sizeof(T);
   const size_t sm_schur = 16 * (128 + 4) * sizeof(T) + 16 * (128 + 4) * sizeof(T);
   { int _r = allow_max_smem((const void*)k_schur<T>); if (_r) return _r; }
-  bool use_tc = false;
+  bool use_tc = false, tc_update = false;
   if constexpr (std::is_same<T, float>::value) {
     const char* e = std::getenv("ORBIT_B200_TC");
     use_tc = f->tc_pack != nullptr && !(e && e[0] == '0');
@@ -1291,6 +1433,14 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
       int _r = allow_max_smem((const void*)k_gemm_tc);
       if (_r) return _r;
       D.tc_min_n = S.tc_min_n;
+      // trailing updates of the blocked pivot LU on the tensor cores as well,
+      // unless ORBIT_B200_TC_UPDATE=0
+      const char* eu = std::getenv("ORBIT_B200_TC_UPDATE");
+      tc_update = !(eu && eu[0] == '0');
+      if (tc_update) {
+        _r = allow_max_smem((const void*)k_update_tc);
+        if (_r) return _r;
+      }
     }
   }
   { int _r = allow_max_smem((const void*)k_prod2<T>); if (_r) return _r; }
@@ -1344,7 +1494,14 @@ int run_factor_t(orbit_factor_s* f, int n_active, double dtau, cudaStream_t st) 
         }
         case FactorLaunch::UPDATE: {
           dim3 g((unsigned)L.items, G);
-          k_update2<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off, L.p0);
+          bool done_tc = false;
+          if constexpr (std::is_same<T, float>::value) {
+            if (use_tc && tc_update) {
+              k_update_tc<<<g, 128, kUpdSmem, st>>>(D, cur, L.item_off, L.p0, f->status);
+              done_tc = true;
+            }
+          }
+          if (!done_tc) k_update2<T><<<g, 256, sm_schur, st>>>(D, cur, L.item_off, L.p0);
           note_launch();
           break;
         }

@@ -78,6 +78,7 @@ struct ChainDev {
   long long spin_limit;
   int never_ready;  // self-test: the first task waits for a count nothing reaches
   int prefetch;     // L2 prefetch of each task's factor rows before its dependency wait
+  int64_t prefetch_bytes;  // at most this many bytes of a task's rows are prefetched
 };
 
 __device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit) {
@@ -484,13 +485,15 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
       constexpr int L = 128 / sizeof(T);
       if (kind == 0) {
         const char* a = reinterpret_cast<const char*>(SQ + (int64_t)it.y * ldn_s);
-        const int64_t bytes = (int64_t)(it.z - it.y) * ldn_s * sizeof(T);
+        const int64_t bytes = min((int64_t)(it.z - it.y) * ldn_s * (int64_t)sizeof(T), D.prefetch_bytes);
         for (int64_t q = (int64_t)tid * 128; q < bytes; q += (int64_t)kSolveThreads * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(a + q));
       } else {
         const int ldm_s = D.ldm[s], m_s = D.m[s];
         const T* Qr = SQ + (int64_t)(n_s + m_s) * ldn_s;
-        for (int i = it.y + (tid >> 3); i < it.z; i += kSolveThreads / 8) {
+        const int64_t row_bytes = (int64_t)(n_s + m_s) * sizeof(T);
+        const int i_end = (int)min((int64_t)it.z, it.y + max((int64_t)1, D.prefetch_bytes / row_bytes));
+        for (int i = it.y + (tid >> 3); i < i_end; i += kSolveThreads / 8) {
           const T* row = SQ + (int64_t)i * ldn_s;
           for (int c = (i & ~(L - 1)) + (tid & 7) * L; c < n_s; c += 8 * L)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(row + c));
@@ -674,7 +677,7 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     if (D.prefetch) {
       if (kind == 0) {
         const char* a = reinterpret_cast<const char*>(SQ + (int64_t)r0 * ldn);
-        const int64_t bytes = (int64_t)(r1 - r0) * ldn * sizeof(T);
+        const int64_t bytes = min((int64_t)(r1 - r0) * ldn * (int64_t)sizeof(T), D.prefetch_bytes);
         for (int64_t q2 = (int64_t)tid * 128; q2 < bytes; q2 += (int64_t)kSolveThreads * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(a + q2));
       }
@@ -1046,7 +1049,7 @@ __device__ __forceinline__ void issue_piece(const T* SQ, int kind, int a, int b,
 }
 
 #ifndef ORBIT_STAGED_MINB
-#define ORBIT_STAGED_MINB 4
+#define ORBIT_STAGED_MINB 8
 #endif
 
 template <typename T, int K>
@@ -1263,7 +1266,7 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
 
 // The staged chain kernel serves the non-transposed sweeps unless
 // ORBIT_B200_CHAIN_STAGED=0; ORBIT_B200_STAGE_KB sets each of its two stage
-// buffers (default 16 KB, at least one staged row).
+// buffers (default 8 KB, at least one staged row).
 bool staged_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("ORBIT_B200_CHAIN_STAGED");
@@ -1275,8 +1278,20 @@ bool staged_enabled() {
 int staged_half_bytes() {
   static const int b = [] {
     const char* e = std::getenv("ORBIT_B200_STAGE_KB");
-    const int kb = e ? std::atoi(e) : 16;
-    return std::min(std::max(kb, 4), 96) * 1024;
+    const int kb = e ? std::atoi(e) : 8;
+    return std::min(std::max(kb, 2), 96) * 1024;
+  }();
+  return b;
+}
+
+// Bytes of each task's factor rows the register-load kernels prefetch into L2
+// before their dependency wait (ORBIT_B200_PREFETCH_KB; 0 or unset: the whole
+// task).
+int64_t prefetch_limit_bytes() {
+  static const int64_t b = [] {
+    const char* e = std::getenv("ORBIT_B200_PREFETCH_KB");
+    const long long kb = e ? std::atoll(e) : 0;
+    return kb > 0 ? (int64_t)kb * 1024 : (int64_t)1 << 40;
   }();
   return b;
 }
@@ -1324,6 +1339,7 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.spin_limit = never_ready ? 20000LL : 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
   D.never_ready = never_ready ? 1 : 0;
   D.prefetch = (sizeof(T) == 4 || B <= 6) ? 1 : 0;
+  D.prefetch_bytes = prefetch_limit_bytes();
   if (D.total <= 0) return ORBIT_OK;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->counters, 0, sizeof(int) * (size_t)f->n_orbits * 16 * S.nsuper, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));

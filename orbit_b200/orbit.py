@@ -59,6 +59,8 @@ class _BinSet:
         self.fb = FactorBatch(sym, 1, lus[0].precision)
         self.fb.numeric([lu.device_stencil() for lu in lus], None, dtau)
         self.N = sym.N
+        for t, lu in enumerate(lus):  # each LU now solves through its bin of this batch
+            lu.attach_to_set(self.fb, t)
 
 
 def _bin_set(lu_list_8) -> _BinSet:
@@ -187,8 +189,13 @@ def solve_orbit_all_species(L_species_per_bin, K_sources_per_bin, emissions_SN, 
     n_species = len(L_species_per_bin[0])
     emissions_SN = np.asarray(emissions_SN, dtype=np.float64)
     if umfpack_sym is None:
-        first = next(L for L in L_species_per_bin[0] if L is not None)
-        umfpack_sym = umfpack_symbolic(first, verbose=verbose)
+        first = next((L for L in L_species_per_bin[0] if L is not None), None)
+        if first is not None:
+            umfpack_sym = umfpack_symbolic(first, verbose=verbose)
+        elif lu_cache:
+            umfpack_sym = next(iter(lu_cache.values())).fb.sym
+        else:
+            raise ValueError("no operator and no LU cache to take the symbolic analysis from; pass umfpack_sym")
     sym = umfpack_sym.sym if isinstance(umfpack_sym, DeviceSymbolic) else umfpack_sym
     dev_orbits = {}  # species -> (9, N) device tensor
     host_orbits = {}  # species -> list of host arrays (seeds and cached copies, returned as given)

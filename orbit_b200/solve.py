@@ -82,7 +82,11 @@ class DeviceLU:
 
     The factorization is done on first use (``solve``), or together with the
     other bins when eight of these are handed to ``solve_orbit_one_species``,
-    which factors them in one batched launch sequence.
+    which factors them in one batched launch sequence; from then on ``solve``
+    uses the batch's factors (a lone factorization made earlier is released),
+    so each LU's factors are held once.  Every ``solve`` moves b and x between
+    host and device, as the reference's duck type takes and returns host
+    arrays.
     """
 
     def __init__(self, L, symbolic, dtau: float = DTAU, precision: int = 64):
@@ -98,6 +102,10 @@ class DeviceLU:
         self.peak_bytes = float(sym.info["front_elems"] * 2 * (8 if precision == 64 else 4))
         self._fb = None
         self._T = None
+        # after a bin-set factorization (solve_orbit_one_species): the batch
+        # holding this LU's factors and its bin there
+        self._set_fb = None
+        self._set_bin = 0
 
     @property
     def nnz(self) -> int:
@@ -109,7 +117,19 @@ class DeviceLU:
             self._T = torch.as_tensor(self.stencil, device="cuda")
         return self._T
 
+    def attach_to_set(self, fb, bin_index: int):
+        """Solve through bin ``bin_index`` of the batch ``fb`` from now on and
+        release this LU's own factorization, if it had one: one set of factors
+        per LU, whichever call factored it first."""
+        self._set_fb = fb
+        self._set_bin = int(bin_index)
+        if self._fb is not None:
+            self._fb.close()
+            self._fb = None
+
     def _factored(self):
+        if self._set_fb is not None:
+            return self._set_fb
         if self._fb is None:
             from .device import FactorBatch
             fb = FactorBatch(self.sym, 1, self.precision, n_sets=1, n_bins=1)
@@ -122,8 +142,9 @@ class DeviceLU:
             raise ValueError(f"trans must be 'N' or 'T'; got {trans!r}")
         import torch
         fb = self._factored()
+        t0 = self._set_bin if self._set_fb is not None else 0
         x = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64), device="cuda")[None]
-        y = fb.chain(x, trans=(trans == "T"), tau0=0, tau1=1, refine=False)
+        y = fb.chain(x, trans=(trans == "T"), tau0=t0, tau1=t0 + 1, refine=False)
         return y[0].cpu().numpy()
 
 

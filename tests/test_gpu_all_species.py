@@ -67,11 +67,14 @@ def test_lu_cache_reused_by_a_second_call():
     L0, L1, rate, emis = _problem()
     K = [{(1, 0): sp.diags(-rate).tocsc()} for _ in range(8)]
     Ls = [[L0[t], L1[t]] for t in range(8)]
-    res = oorb.solve_orbit_all_species(Ls, K, emis, N, tol=1e-12, verbose=False, return_lu_cache=True)
+    from orbit_b200.solve import umfpack_symbolic
+    sym = umfpack_symbolic(L0[0], verbose=False)
+    res = oorb.solve_orbit_all_species(Ls, K, emis, N, tol=1e-12, verbose=False, return_lu_cache=True,
+                                       umfpack_sym=sym)
     assert set(res["lu_cache"]) == {0, 1}
     assert all(Ls[t][s] is None for t in range(8) for s in range(2))  # operators released
     res2 = oorb.solve_orbit_all_species(Ls, K, 2.0 * emis, N, tol=1e-12, verbose=False,
-                                        lu_cache=res["lu_cache"])
+                                        lu_cache=res["lu_cache"], umfpack_sym=sym)
     o0 = _oracle(L0, 2.0 * SPC.emis)
     o1 = _oracle(L1, [0.6 * SPC.emis[t] + rate * o0[t] for t in range(8)])
     assert _rel(np.stack(res2["orbits"][0]), np.stack(o0)) < 1e-9

@@ -36,6 +36,11 @@ def test_lu_objects_and_orbit_dropin():
     assert _rel(lus[2].solve(b), ref.solve(b)) < 1e-12
     assert _rel(lus[2].solve(b, trans="T"), ref.solve(b, trans="T")) < 1e-12
     assert _rel(oorb.apply_monodromy(Z["mono_v"], lus), Z["mono_Mv"]) < 1e-12
+    # the bin-set factorization replaced lus[2]'s own: one set of factors per LU,
+    # and .solve now runs through bin 2 of the batch
+    assert lus[2]._fb is None and lus[2]._set_fb is not None
+    assert _rel(lus[2].solve(b), ref.solve(b)) < 1e-12
+    assert _rel(lus[2].solve(b, trans="T"), ref.solve(b, trans="T")) < 1e-12
     assert _rel(oadj.apply_monodromy_adjoint(Z["mono_v"], lus), Z["mono_MTv"]) < 1e-12
     orbit, info = oorb.solve_orbit_one_species(lus, list(SPC.emis), tol=1e-12)
     assert _rel(np.stack(orbit), Z["orbit"]) < 1e-9
