@@ -731,12 +731,19 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
       k_block_resid<<<gb, kVT, 0, st>>>(Rb, f->E, dtau, Cb, f->A_stencil, sy->d.perm, sy->d.iperm, sy->S.nz,
                                         sy->S.ny, sy->S.nx, d_ids, f->set_of);
       note_launch();
-      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
-      rc = launch_chain(f, B, d_ids, 0, 0, 8, Rb, 1.0, st);
-      if (rc) return rc;
-      for (int o : oact) mv[o]++;
-      k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, f->X + 8 * N, 9 * N, zero, nullptr, 0, d_ids, N);
-      note_launch();
+      if (it == 0 && !warm) {
+        // from c = 0 the residual forcing is dtau e itself, whose sweep is the
+        // s computed above: reuse it
+        k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, c.Sv, c.vs, zero, nullptr, 0, d_ids, N);
+        note_launch();
+      } else {
+        ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+        rc = launch_chain(f, B, d_ids, 0, 0, 8, Rb, 1.0, st);
+        if (rc) return rc;
+        for (int o : oact) mv[o]++;
+        k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, f->X + 8 * N, 9 * N, zero, nullptr, 0, d_ids, N);
+        note_launch();
+      }
       rc = sqnorm(c, c.Dv, c.vs, d_ids, B, S_TMP);
       if (rc) return rc;
       rc = fetch_scal(c);

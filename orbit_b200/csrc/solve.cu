@@ -25,7 +25,6 @@
 
 #include "common.cuh"
 #include "handles.h"
-#include "tc.cuh"
 
 namespace orbit {
 
@@ -79,7 +78,87 @@ struct ChainDev {
   int never_ready;  // self-test: the first task waits for a count nothing reaches
   int prefetch;     // L2 prefetch of each task's factor rows before its dependency wait
   int64_t prefetch_bytes;  // at most this many bytes of a task's rows are prefetched
+  int ngroups;  // task groups (orbits or right-hand-side groups) split into ngroups ...
+  int goff;     // ... whose phase sequences start goff phases apart
 };
+
+// Claim order.  A launch's work is nb bins x nphase phases (fwd leaves->root,
+// bwd root->leaves) for B task groups (single orbits, or groups of
+// right-hand sides).  The groups are split into D.ngroups sets; set gr runs its
+// global phase g = bin * nphase + phase at slot g + gr * D.goff, and tasks are
+// claimed slot by slot (set, then group, then item within a slot).  With one
+// set this is the plain bin / phase / group order; with several, the sets reach
+// the few large tasks at the top of the tree at different times, so tasks of
+// the other sets fill the GPU meanwhile.  Every dependency lies inside one
+// group (earlier phase or bin of the same orbit), so it is still claimed
+// earlier, and the earliest unfinished task can always run.
+constexpr int kMaxSlots = 9 * kMaxPhases + 1;
+constexpr int kMaxSets = 8;
+
+// Shared tables of the claim order: first task of every slot, first group of
+// every set, task count of every phase.
+struct SlotTables {
+  int slot[kMaxSlots];
+  int set_first[kMaxSets + 1];
+  int cnt[kMaxPhases];
+  int nslot, G;
+};
+
+template <typename T>
+__device__ __forceinline__ void build_slots(const ChainDev<T>& D, SlotTables& S) {
+  const int nb = D.total / (D.items_per_bin * D.B);
+  const int G = nb * D.nphase;
+  const int nslot = G + (D.ngroups - 1) * D.goff;
+  for (int i = threadIdx.x; i < D.nphase; i += blockDim.x) S.cnt[i] = D.phase_off[i + 1] - D.phase_off[i];
+  for (int i = threadIdx.x; i <= D.ngroups; i += blockDim.x) S.set_first[i] = (int)(((int64_t)i * D.B) / D.ngroups);
+  __syncthreads();
+  for (int sg = threadIdx.x; sg < nslot; sg += blockDim.x) {
+    int sz = 0;
+    for (int gr = 0; gr < D.ngroups; ++gr) {
+      const int g = sg - gr * D.goff;
+      if (g >= 0 && g < G) sz += S.cnt[g % D.nphase] * (S.set_first[gr + 1] - S.set_first[gr]);
+    }
+    S.slot[sg + 1] = sz;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    S.slot[0] = 0;
+    for (int sg = 1; sg <= nslot; ++sg) S.slot[sg] += S.slot[sg - 1];
+    S.nslot = nslot;
+    S.G = G;
+  }
+  __syncthreads();
+}
+
+// Task t -> bin q (0-based in the launch), phase p, group index gi, item index.
+template <typename T>
+__device__ __forceinline__ void decode_task(const ChainDev<T>& D, const SlotTables& S, int t, int& q, int& p,
+                                            int& gi, int& item) {
+  int lo = 0, hi = S.nslot;  // slot with slot[lo] <= t < slot[lo + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (S.slot[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  int rem = t - S.slot[lo];
+  for (int gr = 0; gr < D.ngroups; ++gr) {
+    const int g = lo - gr * D.goff;
+    if (g < 0 || g >= S.G) continue;
+    const int pp = g % D.nphase;
+    const int cnt = S.cnt[pp];
+    const int sz = cnt * (S.set_first[gr + 1] - S.set_first[gr]);
+    if (rem < sz) {
+      const int k = rem / cnt;
+      q = g / D.nphase;
+      p = pp;
+      gi = S.set_first[gr] + k;
+      item = D.phase_off[pp] + (rem - k * cnt);
+      return;
+    }
+    rem -= sz;
+  }
+  q = p = gi = item = 0;  // not reached for t < total
+}
 
 __device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit) {
   long long it = 0;
@@ -442,10 +521,9 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
   __shared__ int s_task;
   __shared__ int s_ok;   // status word clean at the claim
   __shared__ int s_dep;  // dependency wait succeeded
-  __shared__ int s_phase[kMaxPhases + 1];  // phase offsets x B
+  __shared__ SlotTables s_tab;
   const int tid = threadIdx.x;
-  const int per_bin = D.items_per_bin * D.B;
-  for (int i = tid; i <= D.nphase; i += blockDim.x) s_phase[i] = D.phase_off[i] * D.B;
+  build_slots(D, s_tab);
   for (;;) {
     if (tid == 0) {
       s_task = atomicAdd(D.task_counter, 1);
@@ -454,20 +532,10 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     __syncthreads();
     const int t = s_task;
     if (t >= D.total || !s_ok) break;
-    const int q = t / per_bin;
-    const int r = t - q * per_bin;
+    int q, p, oi, item;
+    decode_task(D, s_tab, t, q, p, oi, item);
     const int tau = D.trans ? (D.tau1 - 1 - q) : (D.tau0 + q);
-    int lo = 0, hi = D.nphase;  // phase p with s_phase[p] <= r < s_phase[p + 1]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (s_phase[mid] <= r) lo = mid;
-      else hi = mid;
-    }
-    const int p = lo;
-    const int rr = r - s_phase[p];
-    const int cnt = D.phase_off[p + 1] - D.phase_off[p];
-    const int oi = rr / cnt;
-    const int4 it = D.items[D.phase_off[p] + (rr - oi * cnt)];
+    const int4 it = D.items[item];
     const int o = D.orbit_ids[oi];
     const int s = it.x, kind = it.w;
     const bool fwd = (kind & 1) == 0;        // kinds 0, 2, 4, 6
@@ -641,10 +709,9 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
   __shared__ int s_task;
   __shared__ int s_ok;   // status word clean at the claim
   __shared__ int s_dep;  // dependency wait succeeded
-  __shared__ int s_phase[kMaxPhases + 1];
+  __shared__ SlotTables s_tab;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int per_bin = D.items_per_bin * D.B;
-  for (int i = tid; i <= D.nphase; i += blockDim.x) s_phase[i] = D.phase_off[i] * D.B;
+  build_slots(D, s_tab);
   for (;;) {
     if (tid == 0) {
       s_task = atomicAdd(D.task_counter, 1);
@@ -653,19 +720,10 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     __syncthreads();
     const int t = s_task;
     if (t >= D.total || !s_ok) break;
-    const int q = t / per_bin;
-    const int r = t - q * per_bin;
+    int q, pph, gi, item;
+    decode_task(D, s_tab, t, q, pph, gi, item);
     const int tau = D.trans ? (D.tau1 - 1 - q) : (D.tau0 + q);
-    int lo = 0, hi = D.nphase;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (s_phase[mid] <= r) lo = mid;
-      else hi = mid;
-    }
-    const int rr = r - s_phase[lo];
-    const int cnt = D.phase_off[lo + 1] - D.phase_off[lo];
-    const int gi = rr / cnt;
-    const int4 it = D.items[D.phase_off[lo] + (rr - gi * cnt)];
+    const int4 it = D.items[item];
     const int s = it.x, kind = it.w, r0 = it.y, r1 = it.z;
     const int nk = min(K, D.Borb - gi * K);
     int o[K];
@@ -900,360 +958,6 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
   }
 }
 
-// ---- staged chain: factor rows moved to shared memory by the TMA engine ----
-//
-// Each task's factor rows are copied global -> shared memory with linear
-// bulk copies (cp.async.bulk, completing on an mbarrier, evict-first in L2)
-// that are issued before the task's dependency wait, so the factor stream
-// is in flight while the task waits for its predecessors and gathers its
-// right-hand side; the dense rows are then multiplied from shared memory.
-// A task's rows are moved in pieces that fit one half of a two-buffer stage:
-// the first two pieces are issued before the wait, each later piece as soon
-// as the buffer it reuses has been consumed.  Rows stage as they are used:
-// forward, row i < n of SQ keeps columns [0, pad4(i)) (the strictly lower
-// part, inv(L11)) and the Pb rows [n, n + m) are one contiguous block;
-// backward, row i keeps the SQ columns [i & ~3, ldn) (inv(U11)) followed by
-// the contiguous Qr rows of the piece.  Non-transposed sweeps only; K
-// right-hand sides per task when every solve slot shares one factor set.
-
-__device__ __forceinline__ int pad4i(int k) { return (k + 3) & ~3; }
-// sum_{k < i} pad4(k)
-__device__ __forceinline__ int64_t pad4_prefix(int i) {
-  if (i <= 1) return 0;
-  const int64_t a = i - 1, g = a >> 2, r = a & 3;
-  return 8 * g * (g + 1) + 4 * r * (g + 1);
-}
-// sum_{k < i} (k & ~3)
-__device__ __forceinline__ int64_t floor4_prefix(int i) {
-  const int64_t g = i >> 2, r = i & 3;
-  return 8 * g * (g - 1) + 4 * r * g;
-}
-// Staged elements of rows [0, i) of a task of the given kind (0 forward, 1 backward).
-__device__ __forceinline__ int64_t staged_prefix(int kind, int i, int n, int ldn, int ldm) {
-  if (kind == 0) return pad4_prefix(min(i, n)) + (int64_t)ldn * max(i - n, 0);
-  return (int64_t)(ldn + (ldm > 0 ? ldm : 0)) * i - floor4_prefix(i);
-}
-
-__device__ __forceinline__ uint64_t l2_evict_first_policy() {
-  uint64_t pol;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
-__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
-                                              uint64_t pol) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
-          tc::smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(tc::smem_u32(bar)), "l"(pol)
-      : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// Dot product of a shared-memory row segment (16-byte aligned at j = 0) with
-// K shared-memory vectors over [j0, j1): G lanes, four 16-byte loads in
-// flight per lane.
-template <typename T, int G, int K>
-__device__ __forceinline__ void dot_seg_smem(const T* a, const T* v, int vcap, int nk, int j0, int j1, int gl,
-                                             T (&acc)[K]) {
-  using V = typename Vec16<T>::type;
-  constexpr int W = Vec16<T>::w;
-  const int ja = min((j0 + W - 1) / W * W, j1);
-  const int jb = max(ja, j1 / W * W);
-  for (int j = j0 + gl; j < ja; j += G) {
-    const T x = a[j];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      if (k < nk) acc[k] = fma(x, v[k * vcap + j], acc[k]);
-  }
-  const V* a4 = reinterpret_cast<const V*>(a);
-  const int nv0 = ja / W, nv1 = jb / W;
-  for (int kk = nv0 + gl; kk < nv1; kk += 2 * G) {
-    const bool b1 = kk + G < nv1;
-    const V x0 = a4[kk];
-    V x1 = {};
-    if (b1) x1 = a4[kk + G];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      if (k < nk) {
-        acc[k] += dot16(x0, v + k * vcap + kk * W);
-        if (b1) acc[k] += dot16(x1, v + k * vcap + (kk + G) * W);
-      }
-  }
-  for (int j = jb + gl; j < j1; j += G) {
-    const T x = a[j];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      if (k < nk) acc[k] = fma(x, v[k * vcap + j], acc[k]);
-  }
-}
-
-struct StagePiece {
-  int a, b;  // rows [a, b) of the task
-};
-
-// Largest b in (a, r1] whose rows [a, b) stage in at most cap elements (every
-// single row fits a half stage by construction of cap).
-__device__ __forceinline__ int piece_end(int kind, int a, int r1, int n, int ldn, int ldm, int64_t cap) {
-  const int64_t base = staged_prefix(kind, a, n, ldn, ldm);
-  int lo = a + 1, hi = r1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (staged_prefix(kind, mid, n, ldn, ldm) - base <= cap) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Issue the bulk copies of rows [a, b) into `buf` (warp 0 only; lane 0 posts
-// the byte count first).
-template <typename T>
-__device__ __forceinline__ void issue_piece(const T* SQ, int kind, int a, int b, int n, int m, int ldn, int ldm,
-                                            T* buf, uint64_t* bar, uint64_t pol) {
-  const int lane = threadIdx.x & 31;
-  const int64_t base = staged_prefix(kind, a, n, ldn, ldm);
-  const int64_t total = staged_prefix(kind, b, n, ldn, ldm) - base;
-  if (lane == 0) {
-    fence_proxy_async_smem();
-    tc::mbar_arrive_expect_tx(bar, (uint32_t)(total * sizeof(T)));
-  }
-  __syncwarp();
-  if (kind == 0) {
-    // SQ rows [a, min(b, n)): columns [0, pad4(i))
-    const int sq_end = min(b, n);
-    for (int i = a + lane; i < sq_end; i += 32) {
-      const int len = pad4i(i);
-      if (len > 0)
-        bulk_g2s_hint(buf + (pad4_prefix(i) - pad4_prefix(a)), SQ + (int64_t)i * ldn, (uint32_t)(len * sizeof(T)),
-                      bar, pol);
-    }
-    const int pa = max(a, n), pb = max(b, n);
-    if (pb > pa && lane == 0) {
-      const int64_t off = pad4_prefix(sq_end) - pad4_prefix(min(a, n));
-      bulk_g2s_hint(buf + off, SQ + (int64_t)pa * ldn, (uint32_t)((int64_t)(pb - pa) * ldn * sizeof(T)), bar, pol);
-    }
-  } else {
-    // SQ rows [a, b): columns [i & ~3, ldn); then the Qr rows [a, b)
-    for (int i = a + lane; i < b; i += 32) {
-      const int c0 = i & ~3;
-      const int64_t off = (int64_t)(i - a) * ldn - (floor4_prefix(i) - floor4_prefix(a));
-      bulk_g2s_hint(buf + off, SQ + (int64_t)i * ldn + c0, (uint32_t)((ldn - c0) * sizeof(T)), bar, pol);
-    }
-    if (m > 0 && lane == 0) {
-      const int64_t off = (int64_t)(b - a) * ldn - (floor4_prefix(b) - floor4_prefix(a));
-      const T* Qr = SQ + (int64_t)(n + m) * ldn;
-      bulk_g2s_hint(buf + off, Qr + (int64_t)a * ldm, (uint32_t)((int64_t)(b - a) * ldm * sizeof(T)), bar, pol);
-    }
-  }
-}
-
-#ifndef ORBIT_STAGED_MINB
-#define ORBIT_STAGED_MINB 8
-#endif
-
-template <typename T, int K>
-__global__ void __launch_bounds__(kSolveThreads, ORBIT_STAGED_MINB) k_chain_staged(ChainDev<T> D, int vcap,
-                                                                                   int half_elems) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  T* stage = reinterpret_cast<T*>(smem_raw);               // 2 x half_elems
-  T* vbuf = stage + 2 * (int64_t)half_elems;                // K vectors of vcap
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ int s_task;
-  __shared__ int s_ok;   // status word clean at the claim
-  __shared__ int s_dep;  // dependency wait succeeded
-  __shared__ int s_phase[kMaxPhases + 1];
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int per_bin = D.items_per_bin * D.B;
-  for (int i = tid; i <= D.nphase; i += blockDim.x) s_phase[i] = D.phase_off[i] * D.B;
-  if (tid == 0) {
-    tc::mbar_init(&bars[0], 1);
-    tc::mbar_init(&bars[1], 1);
-    tc::fence_barrier_init();
-  }
-  __syncthreads();
-  const uint64_t pol = l2_evict_first_policy();
-  uint32_t par0 = 0, par1 = 0;  // next phase parity of each stage buffer
-  constexpr long long kStageWait = 1LL << 24;
-  for (;;) {
-    if (tid == 0) {
-      s_task = atomicAdd(D.task_counter, 1);
-      s_ok = ld_volatile(D.status) == 0;
-    }
-    __syncthreads();
-    const int t = s_task;
-    if (t >= D.total || !s_ok) break;
-    const int q = t / per_bin;
-    const int r = t - q * per_bin;
-    const int tau = D.tau0 + q;
-    int lo = 0, hi = D.nphase;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (s_phase[mid] <= r) lo = mid;
-      else hi = mid;
-    }
-    const int rr = r - s_phase[lo];
-    const int cnt = D.phase_off[lo + 1] - D.phase_off[lo];
-    const int gi = rr / cnt;
-    const int4 it = D.items[D.phase_off[lo] + (rr - gi * cnt)];
-    const int s = it.x, kind = it.w, r0 = it.y, r1 = it.z;
-    const int nk = K == 1 ? 1 : min(K, D.Borb - gi * K);
-    int o[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) o[k] = D.orbit_ids[gi * K + (k < nk ? k : 0)];
-    int* cbase = D.counters + (int64_t)o[0] * 8 * 2 * D.nsuper;
-    const int n = D.n[s], m = D.m[s], first = D.first[s], ldn = D.ldn[s], ldm = D.ldm[s];
-    const int ldm_st = m > 0 ? ldm : 0;
-    const T* SQ = D.factors + ((int64_t)D.set_of[o[0]] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
-    // ---- pieces 0 and 1 in flight before the dependency wait ----
-    int pa = r0, pb = piece_end(kind, r0, r1, n, ldn, ldm_st, half_elems);
-    int pc = pb < r1 ? piece_end(kind, pb, r1, n, ldn, ldm_st, half_elems) : pb;
-    if (warp == 0) {
-      issue_piece<T>(SQ, kind, pa, pb, n, m, ldn, ldm_st, stage, &bars[0], pol);
-      if (pc > pb) issue_piece<T>(SQ, kind, pb, pc, n, m, ldn, ldm_st, stage + half_elems, &bars[1], pol);
-    }
-    // ---- dependencies ----
-    if (tid == 0) {
-      bool ok = true;
-      if (kind == 0) {
-        for (int q2 = 0; q2 < 2 && ok; ++q2) {
-          const int c = D.child[2 * s + q2];
-          if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
-        }
-        if (ok && tau > D.tau0)
-          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
-      } else {
-        const int par = D.parent[s];
-        if (par < 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit);
-        else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
-      }
-      s_dep = ok;
-      __threadfence();
-    }
-    __syncthreads();
-    if (!s_dep) {
-      // leave only once the copies this task issued have landed
-      if (tid == 0) {
-        tc::mbar_wait(&bars[0], par0, kStageWait);
-        if (pc > pb) tc::mbar_wait(&bars[1], par1, kStageWait);
-      }
-      __syncthreads();
-      break;
-    }
-    // ---- right-hand sides over the range the rows read ----
-    const int n0pad = (n + 3) & ~3;
-    if (kind == 0) {
-      const int lo_end = min(r1, n), hi0 = max(r0, n), w = n + m;
-      const int32_t* g0 = D.ginv + D.ginv_off[s];
-      const int32_t* g1 = g0 + w;
-      const int c0 = D.child[2 * s], c1 = D.child[2 * s + 1];
-      for (int k = 0; k < nk; ++k) {
-        T* vec = vbuf + k * vcap;
-        const double* Xin = D.X + ((int64_t)o[k] * 9 + tau) * D.N;
-        const double* Ein = D.E ? D.E + ((int64_t)o[k] * 8 + tau) * D.N : nullptr;
-        const double* Wo = D.W + (int64_t)o[k] * D.w_size;
-        const double* W0 = c0 >= 0 ? Wo + D.woff[c0] : nullptr;
-        const double* W1 = c1 >= 0 ? Wo + D.woff[c1] : nullptr;
-        for (int i = tid; i < lo_end; i += kSolveThreads) {
-          double v = Xin[first + i];
-          if (Ein) v += D.escale * Ein[first + i];
-          const int u0 = g0[i], u1 = g1[i];
-          if (u0 >= 0) v += W0[u0];
-          if (u1 >= 0) v += W1[u1];
-          vec[i] = (T)v;
-        }
-        for (int i = hi0 + tid; i < r1; i += kSolveThreads) {
-          double v = 0.0;
-          const int u0 = g0[i], u1 = g1[i];
-          if (u0 >= 0) v += W0[u0];
-          if (u1 >= 0) v += W1[u1];
-          vec[i] = (T)v;
-        }
-      }
-    } else {
-      const int32_t* ui = D.uidx + D.uoff[s];
-      for (int k = 0; k < nk; ++k) {
-        T* vec = vbuf + k * vcap;
-        const double* Yo = D.Y + (int64_t)o[k] * D.N;
-        const double* Xout = D.X + ((int64_t)o[k] * 9 + tau + 1) * D.N;
-        for (int i = r0 + tid; i < n; i += kSolveThreads) vec[i] = (T)Yo[first + i];
-        for (int u = tid; u < m; u += kSolveThreads) vec[n0pad + u] = (T)Xout[ui[u]];
-      }
-    }
-    __syncthreads();
-    // ---- pieces: wait, multiply, refill the buffer with the piece after next ----
-    const int64_t woff = D.woff[s];
-    int buf = 0;
-    bool ok_stage = true;
-    while (pa < r1) {
-      uint32_t& par = buf == 0 ? par0 : par1;
-      T* sb = stage + (int64_t)buf * half_elems;
-      if (!tc::mbar_wait(&bars[buf], par, kStageWait)) ok_stage = false;
-      par ^= 1u;
-      if (!__syncthreads_and(ok_stage ? 1 : 0)) {
-        if (tid == 0) raise_status(D.status, ORBIT_ERR_TIMEOUT);
-        ok_stage = false;
-        break;
-      }
-      const int64_t base = staged_prefix(kind, pa, n, ldn, ldm_st);
-      if (kind == 0) {
-        const int sq_end = min(pb, n);
-        const int64_t pb_off = pad4_prefix(sq_end) - pad4_prefix(min(pa, n));
-        const int pbase = max(pa, n);
-        auto partial = [&](auto g, int i, int gl, T(&acc)[K]) {
-          if (i < n)
-            dot_seg_smem<T, decltype(g)::value, K>(sb + (pad4_prefix(i) - base), vbuf, vcap, nk, 0, i, gl, acc);
-          else
-            dot_seg_smem<T, decltype(g)::value, K>(sb + pb_off + (int64_t)(i - pbase) * ldn, vbuf, vcap, nk, 0, n,
-                                                   gl, acc);
-        };
-        auto store = [&](int i, T(&acc)[K]) {
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            if (k < nk) {
-              const double y = (double)(vbuf[k * vcap + i] + acc[k]);
-              if (i < n) D.Y[(int64_t)o[k] * D.N + first + i] = y;
-              else D.W[(int64_t)o[k] * D.w_size + woff + (i - n)] = y;
-            }
-        };
-        const int Gl = group_lanes<T>(min(pb - 1, n));
-        ORBIT_GROUPED_ROWS_MULTI(T, K, Gl, pa, pb, warp, kWarps, partial, store);
-      } else {
-        const int64_t qr_off = (int64_t)(pb - pa) * ldn - (floor4_prefix(pb) - floor4_prefix(pa));
-        auto partial = [&](auto g, int i, int gl, T(&acc)[K]) {
-          constexpr int Gv = decltype(g)::value;
-          const int c0 = i & ~3;
-          const T* row = sb + ((int64_t)(i - pa) * ldn - (floor4_prefix(i) - floor4_prefix(pa)));
-          dot_seg_smem<T, Gv, K>(row, vbuf + c0, vcap, nk, i - c0, n - c0, gl, acc);
-          if (m > 0) dot_seg_smem<T, Gv, K>(sb + qr_off + (int64_t)(i - pa) * ldm, vbuf + n0pad, vcap, nk, 0, m, gl, acc);
-        };
-        auto store = [&](int i, T(&acc)[K]) {
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            if (k < nk) D.X[((int64_t)o[k] * 9 + tau + 1) * D.N + first + i] = (double)acc[k];
-        };
-        const int Gl = group_lanes<T>(n - pa + m);
-        ORBIT_GROUPED_ROWS_MULTI(T, K, Gl, pa, pb, warp, kWarps, partial, store);
-      }
-      __syncthreads();  // buffer `buf` consumed
-      pa = pb;
-      pb = pc;
-      if (pb < r1) {
-        pc = piece_end(kind, pb, r1, n, ldn, ldm_st, half_elems);
-        if (warp == 0) issue_piece<T>(SQ, kind, pb, pc, n, m, ldn, ldm_st, sb, &bars[buf], pol);
-      } else {
-        pc = pb;
-      }
-      buf ^= 1;
-    }
-    if (!ok_stage) break;
-    if (tid == 0) {
-      __threadfence();
-      red_release_add(cbase + (tau * 2 + (kind == 0 ? 0 : 1)) * D.nsuper + s, 1);
-    }
-  }
-}
-
 // x[tau0] += escale * E[tau0] (forcing of the transposed chain's last bin)
 __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, int64_t N, int tau0,
                               double escale) {
@@ -1264,36 +968,30 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
     x[i] += escale * e[i];
 }
 
-// The staged chain kernel serves the non-transposed sweeps unless
-// ORBIT_B200_CHAIN_STAGED=0; ORBIT_B200_STAGE_KB sets each of its two stage
-// buffers (default 8 KB, at least one staged row).
-bool staged_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("ORBIT_B200_CHAIN_STAGED");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
-int staged_half_bytes() {
-  static const int b = [] {
-    const char* e = std::getenv("ORBIT_B200_STAGE_KB");
-    const int kb = e ? std::atoi(e) : 8;
-    return std::min(std::max(kb, 2), 96) * 1024;
-  }();
-  return b;
-}
-
-// Bytes of each task's factor rows the register-load kernels prefetch into L2
-// before their dependency wait (ORBIT_B200_PREFETCH_KB; 0 or unset: the whole
-// task).
+// Bytes of each task's factor rows prefetched into L2 before its dependency
+// wait: the first 16 KB (ORBIT_B200_PREFETCH_KB; 0 = the whole task).  With
+// every resident CTA prefetching its whole task (up to 64 KB at the
+// large-batch schedule) the prefetched lines outgrow L2 and are fetched twice
+// (1.5x the algorithmic DRAM traffic at 12 orbits); a 16 KB window keeps them
+// resident and was the fastest window measured (4, 8, 16 KB, whole task).
 int64_t prefetch_limit_bytes() {
   static const int64_t b = [] {
     const char* e = std::getenv("ORBIT_B200_PREFETCH_KB");
-    const long long kb = e ? std::atoll(e) : 0;
+    const long long kb = e ? std::atoll(e) : 16;
     return kb > 0 ? (int64_t)kb * 1024 : (int64_t)1 << 40;
   }();
   return b;
+}
+
+// Sets of task groups whose phase sequences are staggered in the claim
+// order (ORBIT_B200_CHAIN_SETS; 1 = all groups in lockstep).
+int chain_phase_sets() {
+  static const int v = [] {
+    const char* e = std::getenv("ORBIT_B200_CHAIN_SETS");
+    const int k = e ? std::atoi(e) : 1;
+    return std::max(1, std::min(k, kMaxSets));
+  }();
+  return v;
 }
 
 template <typename T>
@@ -1340,6 +1038,8 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.never_ready = never_ready ? 1 : 0;
   D.prefetch = (sizeof(T) == 4 || B <= 6) ? 1 : 0;
   D.prefetch_bytes = prefetch_limit_bytes();
+  D.ngroups = std::max(1, std::min(Bt, chain_phase_sets()));
+  D.goff = D.ngroups > 1 ? std::max(1, D.nphase / D.ngroups) : 0;
   if (D.total <= 0) return ORBIT_OK;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->counters, 0, sizeof(int) * (size_t)f->n_orbits * 16 * S.nsuper, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
@@ -1352,45 +1052,6 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   int dev = 0, sms = 0, occ = 0;
   ORBIT_CUDA_TRY(cudaGetDevice(&dev));
   ORBIT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  if (!trans && !never_ready && S.max_sub_front == 0 && staged_enabled()) {
-    // factor rows staged in shared memory by bulk copies (k_chain_staged)
-    int maxrow = 4;
-    for (int s = 0; s < S.nsuper; ++s)
-      maxrow = std::max(maxrow, S.ldn[s] + (S.m[s] > 0 ? S.ldm[s] : 0));
-    int half = staged_half_bytes() / (int)sizeof(T);
-    half = (std::max(half, maxrow) + 3) & ~3;
-    const int vcap = (S.max_front + 8 + 3) & ~3;
-    const int K = multi ? KM : 1;
-    const size_t ssmem = sizeof(T) * ((size_t)2 * half + (size_t)K * vcap);
-    const void* fn = multi ? (const void*)k_chain_staged<T, KM> : (const void*)k_chain_staged<T, 1>;
-    {
-      int r0 = allow_max_smem(fn);
-      if (r0) return r0;
-    }
-    ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kSolveThreads, ssmem));
-    if (occ < 1) {
-      set_last_error("staged chain kernel cannot be resident (shared memory)");
-      return ORBIT_ERR_INTERNAL;
-    }
-    int grid = sms * occ;
-    if (grid > D.total) grid = D.total;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (f->prof_on) {
-      cudaEventCreate(&e0);
-      cudaEventCreate(&e1);
-      cudaEventRecord(e0, st);
-    }
-    if (multi) k_chain_staged<T, KM><<<grid, kSolveThreads, ssmem, st>>>(D, vcap, half);
-    else k_chain_staged<T, 1><<<grid, kSolveThreads, ssmem, st>>>(D, vcap, half);
-    note_launch();
-    if (f->prof_on) {
-      cudaEventRecord(e1, st);
-      f->prof_chain.push_back({e0, e1});
-      f->prof_chain_bytes += (double)B * (tau1 - tau0) * S.fac_nnz * sizeof(T);
-    }
-    ORBIT_CUDA_TRY(cudaGetLastError());
-    return ORBIT_OK;
-  }
   if (multi) {
     const int vcap = (S.max_front + 8 + 3) & ~3;
     const size_t msmem = sizeof(T) * ((size_t)KM * vcap + (size_t)KM * kWarps * 32);
