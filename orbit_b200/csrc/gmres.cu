@@ -300,6 +300,48 @@ __global__ void k_block_resid(double* R, const double* E, double fs, const doubl
   }
 }
 
+// Block-cyclic residual of the eight transposed bin equations
+// A_tau^T (lam_tau - R_tau) = lam_{tau+1} (lam_8 := lam_0), FP64, permuted
+// order: rho_tau = lam_{tau+1} - A_tau^T (lam_tau - R_tau).  Written in the
+// forcing layout of the transposed chain, which adds E[tau+1] before P_tau^T:
+// Rs[k] = rho_{k-1} for k = 1..7, Rs[0] = 0, and rho_7 (the input of the last
+// bin) into rho7.  L: per orbit 9 vectors (lam_0..lam_7 in slots 0..7);
+// R: per orbit 8 receptors.
+__global__ void k_block_resid_T(double* Rs, double* rho7, int64_t r7s, const double* R, const double* Lb,
+                                const double* Ast, const int32_t* perm, const int32_t* iperm, int nz, int ny,
+                                int nx, const int* ids, const int* set_of) {
+  const int o = ids[blockIdx.y];
+  const int64_t N = (int64_t)nz * ny * nx;
+  const int64_t nxy = (int64_t)nx * ny;
+  const double* L = Lb + (int64_t)o * 9 * N;
+  const double* Ro = R + (int64_t)o * 8 * N;
+  double* Ro_s = Rs + (int64_t)o * 8 * N;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = perm[p];
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+    const int64_t nb[6] = {c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy};
+    const bool has[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+    const int opp[6] = {2, 1, 4, 3, 6, 5};
+    int64_t q[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) q[d] = has[d] ? iperm[nb[d]] : 0;
+    Ro_s[p] = 0.0;
+    for (int tau = 0; tau < 8; ++tau) {
+      const double* A = Ast + ((int64_t)set_of[o] * 8 + tau) * 7 * N;
+      const double* lam = L + (int64_t)tau * N;
+      const double* rr = Ro + (int64_t)tau * N;
+      // (A^T mu)_p = A_pp mu_p + sum over neighbours q of A_qp mu_q, mu = lam - R
+      double acc = A[c] * (lam[p] - rr[p]);
+#pragma unroll
+      for (int d = 0; d < 6; ++d)
+        if (has[d]) acc = fma(A[(int64_t)opp[d] * N + nb[d]], lam[q[d]] - rr[q[d]], acc);
+      const double rho = L[(int64_t)((tau + 1) & 7) * N + p] - acc;
+      if (tau < 7) Ro_s[(int64_t)(tau + 1) * N + p] = rho;
+      else rho7[(int64_t)o * r7s + p] = rho;
+    }
+  }
+}
+
 __global__ void k_count_neg(double* partial, const double* X, int64_t xs, int64_t len, const int* ids) {
   __shared__ double red[kVT / 32];
   const int o = ids[blockIdx.y];
@@ -656,11 +698,11 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
   const double fscale = trans ? 1.0 : dtau;
   std::vector<int> mv(f->n_orbits, 0), iters(f->n_orbits, 0), conv(f->n_orbits, 0), outer(f->n_orbits, 0);
   std::vector<double> rn(f->n_orbits, 0.0);
-  // s = sweep of the forcing from zero.  In the mixed forward solve s only
-  // sets the stopping tolerance (atol = tol ||s||; the block-cyclic refinement
-  // starts from the forcing itself), so one FP32 sweep is enough there: its
-  // norm is exact to ~1e-7 relative.  Every other path sweeps accurately.
-  if (c.mixed && !trans) rc = launch_chain(f, n, d_ids, 0, 0, 8, f->E, fscale, st);
+  // s = sweep of the forcing from zero.  In the mixed solves s only sets the
+  // stopping tolerance (atol = tol ||s||; the block-cyclic refinement starts
+  // from the forcing itself), so one FP32 sweep is enough there: its norm is
+  // exact to ~1e-7 relative.  The FP64 solves sweep exactly.
+  if (c.mixed) rc = launch_chain(f, n, d_ids, trans, 0, 8, f->E, fscale, st);
   else rc = chain_accurate(c, d_ids, n, f->E, fscale);
   if (rc) return rc;
   for (int o = 0; o < n; ++o) mv[o]++;
@@ -801,20 +843,55 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
     note_launch();
     mixed_done = true;
   } else {
-    // outer FP64 refinement of the monodromy residual
+    // Block-cyclic FP64 refinement of the transposed problem, the mirror of the
+    // forward one: the adjoint orbit solves the eight coupled equations
+    // A_tau^T (lam_tau - R_tau) = lam_{tau+1} (lam_8 := lam_0), whose FP64
+    // residual rho needs only stencil products (k_block_resid_T).  A correction
+    // delta solves the same periodic problem with rho as forcing,
+    // delta_tau = P_tau^T (delta_{tau+1} + rho_tau), in FP32: s_rho by one
+    // transposed sweep, GMRES on (I - M~^T), one recovery sweep; the FP64 orbit
+    // accumulates the corrections.  ||s_rho|| is the adjoint residual
+    // ||(I - M^T) lam_0 - s|| of the current orbit.
+    double* Lb = c.XS;                                     // per orbit 9: lam_0..lam_7 in slots 0..7
+    double* Rs = f->tmpv + 15 * N * (int64_t)f->n_orbits;  // per orbit 8: shifted residual forcing
+    double* rho7 = c.Xv;                                   // per orbit: rho_7 (stride vs)
+    ORBIT_CUDA_TRY(cudaMemsetAsync(Lb, 0, sizeof(double) * 9 * N * f->n_orbits, st));
     std::vector<int> oact = act;
-    const int max_outer = 12;
-    for (int it = 0; it < max_outer && !oact.empty(); ++it) {
+    if (warm && !oact.empty()) {
+      // start from the FP32 transposed sweep of the warm start:
+      // lam_tau = X[tau] + R_tau (tau = 1..7), lam_0 = X[0]
+      const int B = (int)oact.size();
+      rc = upload_ids(c, oact, d_ids);
+      if (rc) return rc;
+      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+      k_lincomb<<<vgrid(N, B), kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, c.Xv, c.vs, zero, nullptr, 0, d_ids, N);
+      note_launch();
+      rc = launch_chain(f, B, d_ids, 1, 0, 8, f->E, 1.0, st);
+      if (rc) return rc;
+      for (int t = 0; t < 8; ++t) {
+        k_lincomb<<<vgrid(N, B), kVT, 0, st>>>(Lb + t * N, 9 * N, one, f->X + t * N, 9 * N, t == 0 ? zero : one,
+                                               t == 0 ? nullptr : f->E + t * N, 8 * N, d_ids, N);
+        note_launch();
+      }
+      for (int o : oact) mv[o]++;
+    }
+    const int max_outer = 8;
+    for (int it = 0; it <= max_outer && !oact.empty(); ++it) {
       const int B = (int)oact.size();
       rc = upload_ids(c, oact, d_ids);
       if (rc) return rc;
       const dim3 gb = vgrid(N, B);
-      // r = s - (x - M x) with FP64-refined bins -> Dv
-      rc = matvec(c, c.Xv, c.vs, c.Rv, c.vs, d_ids, B, true);
+      k_block_resid_T<<<gb, kVT, 0, st>>>(Rs, rho7, c.vs, f->E, Lb, f->A_stencil, sy->d.perm, sy->d.iperm, sy->S.nz,
+                                          sy->S.ny, sy->S.nx, d_ids, f->set_of);
+      note_launch();
+      // s_rho: transposed sweep from X[8] = rho_7 with the shifted forcing
+      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+      k_lincomb<<<gb, kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, rho7, c.vs, zero, nullptr, 0, d_ids, N);
+      note_launch();
+      rc = launch_chain(f, B, d_ids, 1, 0, 8, Rs, 1.0, st);
       if (rc) return rc;
-      for (int o : oact) mv[o] += 2;
-      Scal mone{nullptr, 0, 0, -1.0};
-      k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, c.Sv, c.vs, mone, c.Rv, c.vs, d_ids, N);
+      for (int o : oact) mv[o]++;
+      k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, f->X, 9 * N, zero, nullptr, 0, d_ids, N);
       note_launch();
       rc = sqnorm(c, c.Dv, c.vs, d_ids, B, S_TMP);
       if (rc) return rc;
@@ -827,31 +904,51 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
         rn[o] = r;
         if (r <= atol[o]) {
           conv[o] = 1;
-        } else {
+        } else if (it < max_outer) {
           keep.push_back(o);
           itol[o] = std::max(atol[o] * 0.5, 1e-4 * r);
         }
       }
       oact.swap(keep);
       if (oact.empty()) break;
-      // correction: (I - M~) d = r, d0 = 0 ; r lives in Dv, d in Tv? use Dv as b and a fresh x
       const int B2 = (int)oact.size();
       rc = upload_ids(c, oact, d_ids);
       if (rc) return rc;
-      // correction d solves (I - M~) d = r with d0 = 0; GMRES uses Rv/Tv as scratch, so d lives in slot 5
-      std::vector<int> cin(f->n_orbits, 0);
-      std::vector<double> rin(f->n_orbits, 0.0);
-      double* xcorr = f->tmpv + 5 * N;  // spare slot 5 of tmpv
+      double* xcorr = f->tmpv + 5 * N;
       k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(xcorr, c.vs, zero, nullptr, 0, zero, nullptr, 0, d_ids, N);
       note_launch();
-      rc = gmres(c, oact, c.Dv, xcorr, itol, maxiter, false, iters, cin, rin, mv, true);
+      std::vector<int> cin(f->n_orbits, 0);
+      std::vector<double> rin(f->n_orbits, 0.0);
+      rc = gmres(c, oact, c.Dv, xcorr, itol, maxiter, false, iters, cin, rin, mv, true, true);
       if (rc) return rc;
       rc = upload_ids(c, oact, d_ids);
       if (rc) return rc;
-      k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(c.Xv, c.vs, one, c.Xv, c.vs, one, xcorr, c.vs, d_ids, N);
+      // corrections of every bin: recovery sweep from X[8] = delta_0 + rho_7
+      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+      k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, xcorr, c.vs, one, rho7, c.vs, d_ids, N);
       note_launch();
+      rc = launch_chain(f, B2, d_ids, 1, 0, 8, Rs, 1.0, st);
+      if (rc) return rc;
+      for (int o : oact) mv[o]++;
+      for (int t = 0; t < 8; ++t) {
+        k_lincomb<<<vgrid(N, B2), kVT, 0, st>>>(Lb + t * N, 9 * N, one, Lb + t * N, 9 * N, one, f->X + t * N,
+                                                9 * N, d_ids, N);
+        note_launch();
+      }
       for (int o : oact) outer[o]++;
     }
+    // adjoint orbit [lam_0, ..., lam_7, lam_0] into the chain buffer
+    rc = upload_ids(c, all, d_ids);
+    if (rc) return rc;
+    for (int t = 0; t <= 8; ++t) {
+      k_lincomb<<<g, kVT, 0, st>>>(f->X + t * N, 9 * N, one, Lb + (t == 8 ? 0 : t) * N, 9 * N, zero, nullptr, 0,
+                                   d_ids, N);
+      note_launch();
+    }
+    // periodicity from the last residual sweep, as in the forward solve
+    k_lincomb<<<g, kVT, 0, st>>>(c.Tv, c.vs, one, c.Dv, c.vs, zero, nullptr, 0, d_ids, N);
+    note_launch();
+    mixed_done = true;
   }
   // recovery: chain with forcing from x
   rc = upload_ids(c, all, d_ids);

@@ -157,8 +157,17 @@ def test_mixed_precision_within_1e6(dev):
     orb, info = fb.solve(e, tol=1e-8)
     assert _rel(orb.cpu().numpy()[0], Z["orbit"]) < 1e-6
     R = torch.as_tensor(Z["adj_R"], device="cuda")[None]
-    adj, _ = fb.solve_adjoint(R, tol=1e-8)
+    adj, ainfo = fb.solve_adjoint(R, tol=1e-8)
     assert _rel(adj.cpu().numpy()[0], Z["adjoint"]) < 1e-6
+    # the block-cyclic refinement's residual is the adjoint residual, and the
+    # periodic closure holds: lam_8 = lam_0
+    assert ainfo[0, 4] == 1.0 and ainfo[0, 1] <= 1e-8
+    a = adj.cpu().numpy()[0]
+    assert np.array_equal(a[0], a[8])
+    # warm-started from the solution, the refinement stops at its first check
+    adj2, ainfo2 = fb.solve_adjoint(R, lam_warm=adj[:, 0].contiguous(), tol=1e-8)
+    assert _rel(adj2.cpu().numpy()[0], Z["adjoint"]) < 1e-6
+    assert ainfo2[0, 6] <= 1
 
 
 def test_batched_equals_alone(dev):
