@@ -78,6 +78,7 @@ struct ChainDev {
   int never_ready;  // self-test: the first task waits for a count nothing reaches
   int prefetch;     // L2 prefetch of each task's factor rows before its dependency wait
   int64_t prefetch_bytes;  // at most this many bytes of a task's rows are prefetched
+  unsigned spin_ns;  // longest sleep between polls of a completion counter
   int ngroups;  // task groups (orbits or right-hand-side groups) split into ngroups ...
   int goff;     // ... whose phase sequences start goff phases apart
 };
@@ -160,7 +161,10 @@ __device__ __forceinline__ void decode_task(const ChainDev<T>& D, const SlotTabl
   q = p = gi = item = 0;  // not reached for t < total
 }
 
-__device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit) {
+// Bounded spin on a completion counter: sleeps between polls double from
+// 32 ns up to max_ns; `limit` polls at most, then ORBIT_ERR_TIMEOUT.
+__device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, long long limit,
+                                        unsigned max_ns = 1024) {
   long long it = 0;
   unsigned ns = 32;
   while (ld_acquire(p) < target) {
@@ -170,7 +174,7 @@ __device__ __forceinline__ bool wait_ge(const int* p, int target, int* status, l
       return false;
     }
     __nanosleep(ns);
-    if (ns < 1024) ns <<= 1;
+    if (ns < max_ns) ns <<= 1;
   }
   return true;
 }
@@ -574,24 +578,24 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     if (tid == 0) {
       bool ok = true;
       if (D.never_ready && t == 0)
-        ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, 0x7fffffff, D.status, D.spin_limit);
+        ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, 0x7fffffff, D.status, D.spin_limit, D.spin_ns);
       if (!ok) {
       } else if (fwd) {
         if (!subtree)
           for (int q2 = 0; q2 < 2 && ok; ++q2) {
             const int c = D.child[2 * s + q2];
-            if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
+            if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit, D.spin_ns);
           }
         if (ok && !trans && tau > D.tau0)
-          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit, D.spin_ns);
         if (ok && trans && tau < D.tau1 - 1)
-          ok = wait_ge(cbase + ((tau + 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+          ok = wait_ge(cbase + ((tau + 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit, D.spin_ns);
       } else {
         const int par = D.parent[s];
         if (par < 0)
-          ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit);
+          ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit, D.spin_ns);
         else
-          ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
+          ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit, D.spin_ns);
       }
       s_dep = ok;
       __threadfence();
@@ -745,16 +749,16 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
       if (kind == 0 || kind == 2) {
         for (int q2 = 0; q2 < 2 && ok; ++q2) {
           const int c = D.child[2 * s + q2];
-          if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit);
+          if (c >= 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + c, D.nch_f[c], D.status, D.spin_limit, D.spin_ns);
         }
         if (ok && kind == 0 && tau > D.tau0)
-          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+          ok = wait_ge(cbase + ((tau - 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit, D.spin_ns);
         if (ok && kind == 2 && tau < D.tau1 - 1)
-          ok = wait_ge(cbase + ((tau + 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit);
+          ok = wait_ge(cbase + ((tau + 1) * 2 + 1) * D.nsuper + s, D.nch_b[s], D.status, D.spin_limit, D.spin_ns);
       } else {
         const int par = D.parent[s];
-        if (par < 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit);
-        else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit);
+        if (par < 0) ok = wait_ge(cbase + (tau * 2 + 0) * D.nsuper + s, D.nch_f[s], D.status, D.spin_limit, D.spin_ns);
+        else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit, D.spin_ns);
       }
       s_dep = ok;
       __threadfence();
@@ -969,11 +973,12 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
 }
 
 // Bytes of each task's factor rows prefetched into L2 before its dependency
-// wait: the first 16 KB (ORBIT_B200_PREFETCH_KB; 0 = the whole task).  With
-// every resident CTA prefetching its whole task (up to 64 KB at the
-// large-batch schedule) the prefetched lines outgrow L2 and are fetched twice
-// (1.5x the algorithmic DRAM traffic at 12 orbits); a 16 KB window keeps them
-// resident and was the fastest window measured (4, 8, 16 KB, whole task).
+// wait at large batches: the first 16 KB (ORBIT_B200_PREFETCH_KB; 0 = the
+// whole task).  With every resident CTA prefetching its whole task (up to 64
+// KB at the large-batch schedule) the prefetched lines outgrow L2 and are
+// fetched twice (1.5x the algorithmic DRAM traffic at 12 orbits); a 16 KB
+// window keeps them resident and was the fastest window measured at 12 orbits
+// (4, 8, 16 KB, whole task), while at 1 and 4 orbits whole tasks were faster.
 int64_t prefetch_limit_bytes() {
   static const int64_t b = [] {
     const char* e = std::getenv("ORBIT_B200_PREFETCH_KB");
@@ -984,12 +989,24 @@ int64_t prefetch_limit_bytes() {
 }
 
 // Sets of task groups whose phase sequences are staggered in the claim
-// order (ORBIT_B200_CHAIN_SETS; 1 = all groups in lockstep).
+// order (ORBIT_B200_CHAIN_SETS, default 2; 1 = all groups in lockstep):
+// measured 7.49 vs 7.62 ms for the 12-orbit FP32 chain, 12.5 vs 13.3 ms FP64,
+// identical results; 3 and 4 sets were slower.
 int chain_phase_sets() {
   static const int v = [] {
     const char* e = std::getenv("ORBIT_B200_CHAIN_SETS");
-    const int k = e ? std::atoi(e) : 1;
+    const int k = e ? std::atoi(e) : 2;
     return std::max(1, std::min(k, kMaxSets));
+  }();
+  return v;
+}
+
+// Longest sleep between polls of a completion counter (ORBIT_B200_SPIN_NS).
+unsigned chain_spin_ns() {
+  static const unsigned v = [] {
+    const char* e = std::getenv("ORBIT_B200_SPIN_NS");
+    const long k = e ? std::atol(e) : 1024;
+    return (unsigned)std::max(32L, std::min(k, 8192L));
   }();
   return v;
 }
@@ -1037,7 +1054,10 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   D.spin_limit = never_ready ? 20000LL : 4000000LL;  // bounded: a few seconds of sleeps (<= 1 us each)
   D.never_ready = never_ready ? 1 : 0;
   D.prefetch = (sizeof(T) == 4 || B <= 6) ? 1 : 0;
-  D.prefetch_bytes = prefetch_limit_bytes();
+  // the window bounds the prefetch only where the prefetched lines of all
+  // resident CTAs outgrow L2 (large batches); small batches prefetch whole tasks
+  D.prefetch_bytes = Bt > 6 ? prefetch_limit_bytes() : ((int64_t)1 << 40);
+  D.spin_ns = chain_spin_ns();
   D.ngroups = std::max(1, std::min(Bt, chain_phase_sets()));
   D.goff = D.ngroups > 1 ? std::max(1, D.nphase / D.ngroups) : 0;
   if (D.total <= 0) return ORBIT_OK;

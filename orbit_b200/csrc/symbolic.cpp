@@ -515,14 +515,17 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
     Q.chunk_elems = k == 0 ? std::max(256, chunk_elems / 2) : k == 1 ? chunk_elems : 2 * chunk_elems;
     Q.nchunk_fwd.assign(ns, 0); Q.nchunk_bwd.assign(ns, 0);
     Q.nchunk_fwdT.assign(ns, 0); Q.nchunk_bwdT.assign(ns, 0);
+    // Transposed sweeps (kinds 2, 3) work one column per lane: their chunks
+    // hold at least 32 columns so that every lane of a warp has one.
     auto chunk_rows = [&](int s, int kind, int rows, std::function<int64_t(int)> rowlen) {
       int start = 0;
       int cnt = 0;
       int64_t acc = 0;
+      const int min_rows = kind >= 2 ? 32 : 1;
       for (int r = 0; r < rows; ++r) {
         acc += std::max<int64_t>(rowlen(r), 1) + 8;
         bool last = (r == rows - 1);
-        if (acc >= Q.chunk_elems || last || (r + 1 - start) >= 1024) {
+        if ((acc >= Q.chunk_elems && r + 1 - start >= min_rows) || last || (r + 1 - start) >= 1024) {
           Q.sitems.push_back(s); Q.sitems.push_back(start); Q.sitems.push_back(r + 1);
           Q.sitems.push_back(kind);
           start = r + 1;
