@@ -261,6 +261,38 @@ __device__ __forceinline__ int group_lanes(int maxlen) {
     }                                                                       \
   } while (0)
 
+// Column-oriented partial dot products of the transposed sweeps: this warp's
+// share (rows i0 + warp, i0 + warp + kWarps, ... below i1) of
+// sum_i a[i * stride] v_k[i] for nk <= K vectors v_k = v + k * vcap, with
+// four loads in flight (lanes hold consecutive columns, so every row step is
+// one coalesced 128-byte read per warp).
+template <typename T, int K>
+__device__ __forceinline__ void col_dot(const T* __restrict__ a, int64_t stride, int i0, int i1, const T* v,
+                                        int vcap, int nk, T (&acc)[K]) {
+  int i = i0 + (threadIdx.x >> 5);
+  for (; i + 3 * kWarps < i1; i += 4 * kWarps) {
+    const T x0 = __ldg(a + (int64_t)i * stride);
+    const T x1 = __ldg(a + (int64_t)(i + kWarps) * stride);
+    const T x2 = __ldg(a + (int64_t)(i + 2 * kWarps) * stride);
+    const T x3 = __ldg(a + (int64_t)(i + 3 * kWarps) * stride);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) {
+        const T* vk = v + k * vcap;
+        acc[k] = fma(x0, vk[i], acc[k]);
+        acc[k] = fma(x1, vk[i + kWarps], acc[k]);
+        acc[k] = fma(x2, vk[i + 2 * kWarps], acc[k]);
+        acc[k] = fma(x3, vk[i + 3 * kWarps], acc[k]);
+      }
+  }
+  for (; i < i1; i += kWarps) {
+    const T x = __ldg(a + (int64_t)i * stride);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < nk) acc[k] = fma(x, v[k * vcap + i], acc[k]);
+  }
+}
+
 // Forward step of one supernode (L, or U^T when trans) for output rows
 // [r0, r1): gathers its right-hand side (own entries of Xin, plus forcing) and
 // the children's update vectors into `vec`, then one dense GEMV.  Ends with a
@@ -326,15 +358,12 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
     for (int cb = r0; cb < r1; cb += 32) {
       const int c = cb + lane;
-      T acc = T(0);
+      T a1[1] = {T(0)};
       if (c < r1) {
-        if (c < n) {
-          for (int i = warp; i <= c; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
-        } else {
-          const int u = c - n;
-          for (int i = warp; i < n; i += kWarps) acc = fma(__ldg(Qr + (int64_t)i * ldm + u), vec[i], acc);
-        }
+        if (c < n) col_dot<T, 1>(SQ + c, ldn, 0, c + 1, vec, 0, 1, a1);
+        else col_dot<T, 1>(Qr + (c - n), ldm, 0, n, vec, 0, 1, a1);
       }
+      const T acc = a1[0];
       red[warp * 32 + lane] = acc;
       __syncthreads();
       if (warp == 0 && c < r1) {
@@ -386,11 +415,12 @@ __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
     const T* Pb = SQ + (int64_t)n * ldn;
     for (int cb = r0; cb < r1; cb += 32) {
       const int c = cb + lane;
-      T acc = T(0);
+      T a1[1] = {T(0)};
       if (c < r1) {
-        for (int i = c + 1 + warp; i < n; i += kWarps) acc = fma(__ldg(SQ + (int64_t)i * ldn + c), vec[i], acc);
-        for (int u = warp; u < m; u += kWarps) acc = fma(__ldg(Pb + (int64_t)u * ldn + c), vec[n0pad + u], acc);
+        col_dot<T, 1>(SQ + c, ldn, c + 1, n, vec, 0, 1, a1);
+        col_dot<T, 1>(Pb + c, ldn, 0, m, vec + n0pad, 0, 1, a1);
       }
+      const T acc = a1[0];
       red[warp * 32 + lane] = acc;
       __syncthreads();
       if (warp == 0 && c < r1) {
@@ -808,22 +838,8 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
 #pragma unroll
         for (int k = 0; k < K; ++k) acc[k] = T(0);
         if (c < r1) {
-          if (c < n) {
-            for (int i = warp; i <= c; i += kWarps) {
-              const T x = __ldg(SQ + (int64_t)i * ldn + c);
-#pragma unroll
-              for (int k = 0; k < K; ++k)
-                if (k < nk) acc[k] = fma(x, vbuf[k * vcap + i], acc[k]);
-            }
-          } else {
-            const int u = c - n;
-            for (int i = warp; i < n; i += kWarps) {
-              const T x = __ldg(Qr + (int64_t)i * ldm + u);
-#pragma unroll
-              for (int k = 0; k < K; ++k)
-                if (k < nk) acc[k] = fma(x, vbuf[k * vcap + i], acc[k]);
-            }
-          }
+          if (c < n) col_dot<T, K>(SQ + c, ldn, 0, c + 1, vbuf, vcap, nk, acc);
+          else col_dot<T, K>(Qr + (c - n), ldm, 0, n, vbuf, vcap, nk, acc);
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) red[(k * kWarps + warp) * 32 + lane] = acc[k];
@@ -859,18 +875,8 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
 #pragma unroll
         for (int k = 0; k < K; ++k) acc[k] = T(0);
         if (c < r1) {
-          for (int i = c + 1 + warp; i < n; i += kWarps) {
-            const T x = __ldg(SQ + (int64_t)i * ldn + c);
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k < nk) acc[k] = fma(x, vbuf[k * vcap + i], acc[k]);
-          }
-          for (int u = warp; u < m; u += kWarps) {
-            const T x = __ldg(Pb + (int64_t)u * ldn + c);
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k < nk) acc[k] = fma(x, vbuf[k * vcap + n0pad + u], acc[k]);
-          }
+          col_dot<T, K>(SQ + c, ldn, c + 1, n, vbuf, vcap, nk, acc);
+          col_dot<T, K>(Pb + c, ldn, 0, m, vbuf + n0pad, vcap, nk, acc);
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) red[(k * kWarps + warp) * 32 + lane] = acc[k];
@@ -1001,11 +1007,13 @@ int chain_phase_sets() {
   return v;
 }
 
-// Longest sleep between polls of a completion counter (ORBIT_B200_SPIN_NS).
+// Longest sleep between polls of a completion counter (ORBIT_B200_SPIN_NS,
+// default 256 ns: 2.65 vs 2.77 ms for a single-orbit FP64 chain against a
+// 1 us cap, no change at 12 orbits; 4 us was slower).
 unsigned chain_spin_ns() {
   static const unsigned v = [] {
     const char* e = std::getenv("ORBIT_B200_SPIN_NS");
-    const long k = e ? std::atol(e) : 1024;
+    const long k = e ? std::atol(e) : 256;
     return (unsigned)std::max(32L, std::min(k, 8192L));
   }();
   return v;
