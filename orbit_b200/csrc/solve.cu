@@ -17,6 +17,12 @@
 // earliest unfinished task can always run.  A wait that exceeds its
 // iteration limit sets ORBIT_ERR_TIMEOUT in the status word and every CTA
 // leaves the loop.
+//
+// Ordering: a task's results are written by all its threads, then a block
+// barrier, then one thread's red.release.gpu on the completion counter; the
+// consumer's thread polls with ld.acquire.gpu, then a block barrier, then all
+// its threads read.  Release and acquire are cumulative over the barriers'
+// CTA-scope ordering, so no separate fence is needed on either side.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,10 +41,10 @@ namespace {
 #endif
 // CTAs per SM the chain kernels are compiled for, per precision: FP32 at 10
 // (48 registers) hides more of the per-task latency than at 8 (64 registers),
-// 4 % faster on a 12-orbit chain even with the few spills it costs; FP64
-// stays at 8, where the single-orbit FP64 solve is fastest
+// 4 % faster on a 12-orbit chain even with the few spills it costs; FP64 at 7
+// (72 registers), which holds twelve 16-byte loads per lane in flight
 #ifndef ORBIT_SOLVE_MINB
-#define ORBIT_SOLVE_MINB 8
+#define ORBIT_SOLVE_MINB 7
 #endif
 #ifndef ORBIT_SOLVE_MINB_FP32
 #define ORBIT_SOLVE_MINB_FP32 10
@@ -192,11 +198,25 @@ __device__ __forceinline__ double dot16(const double2& a, const double* v) {
   return a.x * v[0] + a.y * v[1];
 }
 
+// 16-byte loads in flight per lane in the row dot products of the chained
+// solves, per precision.  Measured on the 80x72x15 grid (8 bins, CUDA events):
+// FP32, 12 orbits at 10 CTAs per SM: 7.21 ms at 4, 6.94 at 6, 7.05 at 7 (8 at
+// 8 CTAs per SM: 7.55); FP64 at 7 CTAs per SM, 1 / 12 orbits: 1.76 / 9.83 ms
+// at 12 (2.44 ms / - at 4 and 8 CTAs per SM; 1.81 / 10.9 at 10; 1.81 / 11.1
+// at 16 and 6 CTAs per SM).
+#ifndef ORBIT_SOLVE_DEPTH_FP32
+#define ORBIT_SOLVE_DEPTH_FP32 6
+#endif
+#ifndef ORBIT_SOLVE_DEPTH_FP64
+#define ORBIT_SOLVE_DEPTH_FP64 12
+#endif
+template <typename T> struct Depth { static constexpr int value = sizeof(T) == 4 ? ORBIT_SOLVE_DEPTH_FP32 : ORBIT_SOLVE_DEPTH_FP64; };
+
 // Per-lane partial of sum_{j0 <= j < j1} a[j] v[j] for a group of G lanes
 // (gl = lane within the group; a 16-byte aligned at j = 0, v in shared memory,
-// 16-byte aligned).  16-byte loads, up to four in flight per lane: the
-// unrolled loop issues its guarded loads before it uses any of them.
-template <typename T, int G = 32>
+// 16-byte aligned).  16-byte loads, up to U in flight per lane: the unrolled
+// loop issues its guarded loads before it uses any of them.
+template <typename T, int G = 32, int U = Depth<T>::value>
 __device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0, int j1, int gl) {
   using V = typename Vec16<T>::type;
   constexpr int W = Vec16<T>::w;
@@ -208,17 +228,22 @@ __device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0
   for (int j = j0 + gl; j < ja; j += G) acc0 = fma(__ldg(a + j), v[j], acc0);
   const int nv0 = ja / W, nv1 = jb / W;
   const V* a4 = reinterpret_cast<const V*>(a);
-  for (int k = nv0 + gl; k < nv1; k += 4 * G) {
-    const bool b1 = k + G < nv1, b2 = k + 2 * G < nv1, b3 = k + 3 * G < nv1;
-    V x1 = {}, x2 = {}, x3 = {};
-    const V x0 = __ldg(a4 + k);
-    if (b1) x1 = __ldg(a4 + k + G);
-    if (b2) x2 = __ldg(a4 + k + 2 * G);
-    if (b3) x3 = __ldg(a4 + k + 3 * G);
-    acc0 += dot16(x0, v + k * W);
-    if (b1) acc1 += dot16(x1, v + (k + G) * W);
-    if (b2) acc2 += dot16(x2, v + (k + 2 * G) * W);
-    if (b3) acc3 += dot16(x3, v + (k + 3 * G) * W);
+  for (int k = nv0 + gl; k < nv1; k += U * G) {
+    V x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      x[u] = V{};
+      if (u == 0 || k + u * G < nv1) x[u] = __ldg(a4 + k + u * G);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (u == 0 || k + u * G < nv1) {
+        const T d = dot16(x[u], v + (k + u * G) * W);
+        if ((u & 3) == 0) acc0 += d;
+        else if ((u & 3) == 1) acc1 += d;
+        else if ((u & 3) == 2) acc2 += d;
+        else acc3 += d;
+      }
   }
   for (int j = jb + gl; j < j1; j += G) acc1 = fma(__ldg(a + j), v[j], acc1);
   return (acc0 + acc1) + (acc2 + acc3);
@@ -243,12 +268,12 @@ __device__ __forceinline__ void grouped_rows(int r0, int r1, int wid, int nw, P&
   }
 }
 
-// Lanes per row from the longest row of the range: about four 16-byte
-// vectors per lane, between 4 and 32 lanes.
-template <typename T>
+// Lanes per row from the longest row of the range: about U 16-byte vectors
+// per lane (U loads in flight), between 4 and 32 lanes.
+template <typename T, int U = 4>
 __device__ __forceinline__ int group_lanes(int maxlen) {
   const int nv = (maxlen + Vec16<T>::w - 1) / Vec16<T>::w;
-  return nv <= 16 ? 4 : nv <= 32 ? 8 : nv <= 64 ? 16 : 32;
+  return nv <= 4 * U ? 4 : nv <= 8 * U ? 8 : nv <= 16 * U ? 16 : 32;
 }
 
 #define ORBIT_GROUPED_ROWS(T, G_, r0, r1, wid, nw, partial, store)           \
@@ -351,7 +376,7 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
       if (i < n) Yo[first + i] = (double)(vec[i] + acc);
       else Wo[woff + (i - n)] = (double)(vec[i] + acc);
     };
-    const int G = group_lanes<T>(min(r1 - 1, n));
+    const int G = group_lanes<T, Depth<T>::value>(min(r1 - 1, n));
     ORBIT_GROUPED_ROWS(T, G, r0, r1, warp, kWarps, partial, store);
   } else {
     // columns of [upper(SQ) | Qr]
@@ -408,7 +433,7 @@ __device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
              dot_seg<T, G>(Qr + (int64_t)i * ldm, vec + n0pad, 0, m, gl);
     };
     auto store = [&](int i, T acc) { Xout[first + i] = (double)acc; };
-    const int G = group_lanes<T>(n - r0 + m);
+    const int G = group_lanes<T, Depth<T>::value>(n - r0 + m);
     ORBIT_GROUPED_ROWS(T, G, r0, r1, warp, kWarps, partial, store);
   } else {
     // columns of [SQ_strict_lower ; Pb] with unit diagonal
@@ -628,7 +653,6 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
           ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit, D.spin_ns);
       }
       s_dep = ok;
-      __threadfence();
     }
     __syncthreads();
     if (!s_dep) break;
@@ -658,7 +682,6 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
       }
     }
     if (tid == 0) {
-      __threadfence();
       red_release_add(cbase + (tau * 2 + (fwd ? 0 : 1)) * D.nsuper + s, 1);
     }
   }
@@ -791,7 +814,6 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
         else ok = wait_ge(cbase + (tau * 2 + 1) * D.nsuper + par, D.nch_b[par], D.status, D.spin_limit, D.spin_ns);
       }
       s_dep = ok;
-      __threadfence();
     }
     __syncthreads();
     if (!s_dep) break;
@@ -962,7 +984,6 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     }
     __syncthreads();
     if (tid == 0) {
-      __threadfence();
       red_release_add(cbase + (tau * 2 + ((kind == 0 || kind == 2) ? 0 : 1)) * D.nsuper + s, 1);
     }
   }
