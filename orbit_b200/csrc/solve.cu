@@ -323,8 +323,8 @@ __device__ __forceinline__ void col_dot(const T* __restrict__ a, int64_t stride,
 // the children's update vectors into `vec`, then one dense GEMV.  Ends with a
 // block barrier.
 template <typename T>
-__device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
-                         T* vec, T* red) {
+__device__ __forceinline__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
+                                         T* vec, T* red) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t N = D.N;
   const int n = D.n[s], m = D.m[s], first = D.first[s];
@@ -409,8 +409,8 @@ __device__ void fwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, in
 // starts at the next 4-element boundary after the own part so both segments
 // can be read with 16-byte loads.  Ends with a block barrier.
 template <typename T>
-__device__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
-                         T* vec, T* red) {
+__device__ __forceinline__ void bwd_node(const ChainDev<T>& D, int o, int tau, int s, int r0, int r1, bool trans,
+                                         T* vec, T* red) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t N = D.N;
   const int n = D.n[s], m = D.m[s], first = D.first[s];
@@ -572,7 +572,10 @@ __device__ void bwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
   __syncwarp();
 }
 
-template <typename T>
+// One instantiation per sweep direction (TR: transposed) and per schedule
+// kind (SUB: the schedule has whole-subtree tasks), so that each kernel
+// carries only the code its tasks run.
+template <typename T, bool TR, bool SUB>
 __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MINB_FP32 : ORBIT_SOLVE_MINB) k_chain(ChainDev<T> D) {
   extern __shared__ unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);      // kWarps * 32
@@ -593,13 +596,13 @@ __global__ void __launch_bounds__(kSolveThreads, sizeof(T) == 4 ? ORBIT_SOLVE_MI
     if (t >= D.total || !s_ok) break;
     int q, p, oi, item;
     decode_task(D, s_tab, t, q, p, oi, item);
-    const int tau = D.trans ? (D.tau1 - 1 - q) : (D.tau0 + q);
+    const int tau = TR ? (D.tau1 - 1 - q) : (D.tau0 + q);
     const int4 it = D.items[item];
     const int o = D.orbit_ids[oi];
     const int s = it.x, kind = it.w;
     const bool fwd = (kind & 1) == 0;        // kinds 0, 2, 4, 6
-    const bool trans = kind == 2 || kind == 3 || kind == 6 || kind == 7;
-    const bool subtree = kind >= 4;
+    const bool trans = TR;                   // kinds 2, 3, 6, 7
+    const bool subtree = SUB && kind >= 4;
     int* cbase = D.counters + (int64_t)o * 8 * 2 * D.nsuper;
     // The factor rows of a row-chunk task do not depend on other tasks: ask L2
     // for them before waiting (forward: whole rows of [SQ; Pb]; backward: the
@@ -1094,8 +1097,11 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
   const size_t smem =
       sizeof(T) * ((size_t)kWarps * 32 + std::max<size_t>(S.max_front + 8, (size_t)kWarps * ((S.max_sub_front + 7) & ~3)) + 8);
+  const bool sub = S.max_sub_front > 0;
+  const void* kfn = trans ? (sub ? (const void*)k_chain<T, true, true> : (const void*)k_chain<T, true, false>)
+                          : (sub ? (const void*)k_chain<T, false, true> : (const void*)k_chain<T, false, false>);
   {
-    int r0 = allow_max_smem((const void*)k_chain<T>);
+    int r0 = allow_max_smem(kfn);
     if (r0) return r0;
   }
   int dev = 0, sms = 0, occ = 0;
@@ -1137,7 +1143,7 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
     }
     return ORBIT_OK;
   }
-  ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_chain<T>, kSolveThreads, smem));
+  ORBIT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kSolveThreads, smem));
   if (occ < 1) {
     set_last_error("chain kernel cannot be resident");
     return ORBIT_ERR_INTERNAL;
@@ -1150,7 +1156,13 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
   }
-  k_chain<T><<<grid, kSolveThreads, smem, st>>>(D);
+  if (trans) {
+    if (sub) k_chain<T, true, true><<<grid, kSolveThreads, smem, st>>>(D);
+    else k_chain<T, true, false><<<grid, kSolveThreads, smem, st>>>(D);
+  } else {
+    if (sub) k_chain<T, false, true><<<grid, kSolveThreads, smem, st>>>(D);
+    else k_chain<T, false, false><<<grid, kSolveThreads, smem, st>>>(D);
+  }
   note_launch();
   if (f->prof_on) {
     cudaEventRecord(e1, st);
