@@ -1003,16 +1003,16 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
 }
 
 // Bytes of each task's factor rows prefetched into L2 before its dependency
-// wait at large batches: the first 16 KB (ORBIT_B200_PREFETCH_KB; 0 = the
-// whole task).  With every resident CTA prefetching its whole task (up to 64
-// KB at the large-batch schedule) the prefetched lines outgrow L2 and are
-// fetched twice (1.5x the algorithmic DRAM traffic at 12 orbits); a 16 KB
-// window keeps them resident and was the fastest window measured at 12 orbits
-// (4, 8, 16 KB, whole task), while at 1 and 4 orbits whole tasks were faster.
+// wait at large batches: the first 32 KB (ORBIT_B200_PREFETCH_KB; 0 = the
+// whole task).  With every resident CTA prefetching whole backward tasks (up
+// to 64 KB at the large-batch schedule) the prefetched lines can outgrow L2
+// and be fetched twice; at 12 orbits the 12-orbit FP32 chain took 6.58 ms with
+// a 32 KB window, 6.66 with 16 KB and 6.76 with 8 KB, while at 1 and 4 orbits
+// whole tasks were fastest.
 int64_t prefetch_limit_bytes() {
   static const int64_t b = [] {
     const char* e = std::getenv("ORBIT_B200_PREFETCH_KB");
-    const long long kb = e ? std::atoll(e) : 16;
+    const long long kb = e ? std::atoll(e) : 32;
     return kb > 0 ? (int64_t)kb * 1024 : (int64_t)1 << 40;
   }();
   return b;
