@@ -82,6 +82,14 @@ typedef struct {
                              weights are 1 and the transport block is not put in
                              concentration form (operator.py:341, fct.py:451-454,
                              operator.py:626); 0 (default) for the concentration form */
+  int periodic_lon;       /* GridData.periodic_lon (nx >= 3): cells i = nx-1 and
+                             i = 0 share the wrap face and the x-boundary loss is
+                             absent (convdiff.py:150-216); the stencil's W entry of
+                             i = 0 and E entry of i = nx-1 are the wrap couplings */
+  const double* u_wrap;       /* UAvg_wrap, (nz, ny); periodic grids only */
+  const double* u_plus_wrap;  /* UAvg_plus_wrap, (nz, ny); split mode */
+  const double* u_minus_wrap; /* UAvg_minus_wrap, (nz, ny); split mode */
+  const double* kmu_wrap;     /* K_meander_u_wrap, (nz, ny); non-split mode, may be NULL */
 } orbit_met_t;
 
 /* Symbolic analysis of one (nz, ny, nx) domain: geometric nested dissection
@@ -100,6 +108,13 @@ int orbit_symbolic_create(int nz, int ny, int nx, int leaf_cells, orbit_symbolic
  * (orbit/core/solve.py:88-207: ordering, qinit). */
 int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_elems, int tc_min_n,
                              int subtree_div, orbit_symbolic_t* out);
+/* orbit_symbolic_create_ex for a grid that may be periodic in longitude
+ * (GridData.periodic_lon, orbit/core/grid_data.py:426-445; needs nx >= 3):
+ * the pattern then has the wrap-face couplings of cells i = 0 and i = nx - 1
+ * (convdiff.py:150-202), which the dissection separates by cutting the
+ * longitude ring with two planes. */
+int orbit_symbolic_create_grid(int nz, int ny, int nx, int periodic_x, int leaf_cells, int chunk_elems,
+                               int tc_min_n, int subtree_div, orbit_symbolic_t* out);
 /* Replaces umfpack_free_symbolic (orbit/core/solve.py:291-296). */
 int orbit_symbolic_destroy(orbit_symbolic_t sym);
 /* info[0..14] = N, nsuper, nlevels, factor nnz (sum n^2+2nm), factor
@@ -133,6 +148,14 @@ int orbit_symbolic_array(orbit_symbolic_t sym, const char* name, void* dst, int6
  * assemble_cmfmc_transport (convection.py:25-140). */
 int orbit_assemble_transport(int nz, int ny, int nx, const orbit_met_t* met,
                              double* T_stencil, double* rowsum, orbit_stream_t stream);
+/* Lateral boundary loss rate of every cell (device, N doubles, >= 0, zero
+ * inside the domain): the open-outflow terms of the transport block's
+ * diagonal at the x (non-periodic grids) and y edges.  Replaces
+ * compute_lateral_boundary_loss (orbit/core/operator.py:25-178), the second
+ * result of assemble_transport_block(..., return_boundary_fluxes=True)
+ * (operator.py:344-347). */
+int orbit_transport_boundary_loss(int nz, int ny, int nx, const orbit_met_t* met, double* loss,
+                                  orbit_stream_t stream);
 
 /* Per-cell species fields of one bin for the species operators (device
  * pointers; (nz, ny, nx) doubles unless noted; NULL where marked optional).
@@ -243,6 +266,16 @@ int orbit_vec_combine(int64_t n, int m, const double* coef, const double* const*
 int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c_base,
                               double dt, double* stencil, orbit_stream_t stream);
 
+/* orbit_fct_source with a lateral-inflow field: c_ghost (device, n_vec x N,
+ * one per vector) holds the boundary inflow concentration c_bc, whose values
+ * in the edge cells stand for the cells beyond each lateral edge: the
+ * far-upwind values of the edge faces (which then keep their van Leer
+ * reconstruction instead of dropping to first order) and the outside
+ * neighbours of the Zalesak bounds.  Replaces compute_horizontal_fct_source
+ * with c_ghost_flat (orbit/core/fct.py:459-492, 283-292, 381-400). */
+int orbit_fct_source_ghost(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
+                           const double* c_ghost, double dt, int limited, double* d, orbit_stream_t stream);
+
 /* y_v = beta y_v + alpha S_v x_v, or S_v^T x_v when trans, for n_vec 7-point
  * stencils (device, n_vec x 7 x N) and vectors (device, n_vec x N): the
  * products L_AD c_{tau+1} of the marginal FCT outer iteration and their
@@ -250,6 +283,13 @@ int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, in
  * apply the same operators as scipy CSC products). */
 int orbit_stencil_apply(int nz, int ny, int nx, int n_vec, const double* stencils, const double* x, double alpha,
                         double beta, int trans, double* y, orbit_stream_t stream);
+/* orbit_stencil_apply on a grid that may be periodic in longitude: with
+ * periodic_x (nx >= 3) the W entry of a cell in column 0 couples it to
+ * column nx - 1 and the E entry of column nx - 1 to column 0, the wrap-face
+ * entries of assemble_horizontal_convdiff (convdiff.py:150-202). */
+int orbit_stencil_apply_grid(int nz, int ny, int nx, int periodic_x, int n_vec, const double* stencils,
+                             const double* x, double alpha, double beta, int trans, double* y,
+                             orbit_stream_t stream);
 
 /* K2 without device allocation, for callers that cannot allocate device
  * memory at the point where they apply the FCT correction (a host model that

@@ -4,7 +4,9 @@ TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).  Restates:
 
 * ``_patankar_A``                         orbit/core/convdiff.py:16-39
 * ``assemble_horizontal_convdiff``        orbit/core/convdiff.py:42-387
-  (non-periodic grids; split and non-split flux modes)
+  (split and non-split flux modes; the periodic-longitude wrap face,
+  convdiff.py:150-202)
+* ``compute_lateral_boundary_loss``       orbit/core/operator.py:25-178
 * ``interface_omega`` +
   ``assemble_vertical_advection``         orbit/core/advection.py:383-523
 * ``assemble_vertical_diffusion``         orbit/core/mixing.py:14-117
@@ -71,8 +73,23 @@ def _face_rate(K_l, K_r, kmeander, u_face, adv_l, adv_r, d, split):
     return diff + adv_l, diff + adv_r
 
 
+def _wrap_face(g, split):
+    """Face rates and terrain ratios of the periodic wrap face between column
+    nx-1 (L) and column 0 (R) (convdiff.py:150-202)."""
+    d = np.broadcast_to(g.dx[None, :], (g.nz, g.ny))
+    uw = g.u_wrap
+    up = g.u_plus_wrap if split else np.maximum(uw, 0.0)
+    um = g.u_minus_wrap if split else np.maximum(-uw, 0.0)
+    km = g.kmu_wrap if g.kmu_wrap is not None else np.zeros_like(uw)
+    rl, rr = _face_rate(g.kxxyy[:, :, -1], g.kxxyy[:, :, 0], km, uw, up / d, um / d, d, split)
+    pl, pr = g.dP[:, :, -1], g.dP[:, :, 0]
+    face = 0.5 * (pl + pr)
+    ok = (pl > 0) & (pr > 0)
+    return rl, rr, np.where(ok, face / pr, 1.0), np.where(ok, face / pl, 1.0)
+
+
 def horizontal_convdiff(g):
-    """Pressure-form horizontal block T_hcd (convdiff.py:42-387, non-periodic)."""
+    """Pressure-form horizontal block T_hcd (convdiff.py:42-387)."""
     nz, ny, nx = g.nz, g.ny, g.nx
     N = nz * ny * nx
     idx = np.arange(N).reshape(nz, ny, nx)
@@ -97,12 +114,15 @@ def horizontal_convdiff(g):
         coo.add(idx[:, :, 1:], idx[:, :, :-1], -(rl * trr))
         diag[:, :, :-1] += rl * trl
         coo.add(idx[:, :, :-1], idx[:, :, 1:], -(rr * trl))
-    # open x boundaries (convdiff.py:204-255): west outflow u- ; east outflow u+ at the outer face
-    w_out = um_all[:, :, 0]
-    diag[:, :, 0] += np.where(w_out > 0, w_out / dx3[:, :, 0], 0.0)
-    e_out = (g.u_plus_e if split else g.u_e)
-    e_cond = e_out > 0 if split else e_out >= 0
-    diag[:, :, -1] += np.where(e_cond, e_out / dx3[:, :, -1], 0.0)
+    if getattr(g, "periodic_lon", False) and nx > 1:
+        # wrap face (convdiff.py:150-202): cell 0 is R, cell nx-1 is L
+        rl, rr, trr, trl = _wrap_face(g, split)
+        diag[:, :, 0] += rr * trr
+        coo.add(idx[:, :, 0], idx[:, :, -1], -(rl * trr))
+        diag[:, :, -1] += rl * trl
+        coo.add(idx[:, :, -1], idx[:, :, 0], -(rr * trl))
+    else:
+        diag += lateral_boundary_loss(g, x_only=True).reshape(nz, ny, nx)
     dy = g.dy
     if ny > 1:
         rl, rr = _face_rate(g.kxxyy[:, :-1, :], g.kxxyy[:, 1:, :], g.kmv[:, 1:, :],
@@ -119,18 +139,39 @@ def horizontal_convdiff(g):
         diag[:, :-1, :] += rl * trs
         coo.add(idx[:, :-1, :], idx[:, 1:, :], -(rr * trs))
     # open y boundaries with the outer-face dx correction (convdiff.py:290-359)
-    lat_s = g.lat[0] - g.dlat / 2.0
-    lat_n = g.lat[-1] + g.dlat / 2.0
-    tr_s = EARTH_RADIUS * np.cos(lat_s * DEG_TO_RAD) * g.dlon * DEG_TO_RAD / g.dx[0]
-    tr_n = EARTH_RADIUS * np.cos(lat_n * DEG_TO_RAD) * g.dlon * DEG_TO_RAD / g.dx[-1]
-    s_out = vm_all[:, 0, :]
-    diag[:, 0, :] += np.where(s_out > 0, s_out / dy * tr_s, 0.0)
-    n_out = (g.v_plus_n if split else g.v_n)
-    n_cond = n_out > 0 if split else n_out >= 0
-    diag[:, -1, :] += np.where(n_cond, n_out / dy * tr_n, 0.0)
+    diag += lateral_boundary_loss(g, y_only=True).reshape(nz, ny, nx)
     pos = diag > 0
     coo.add(idx[pos], idx[pos], diag[pos])
     return coo.csc()
+
+
+def lateral_boundary_loss(g, x_only=False, y_only=False):
+    """Open-outflow loss rate of the lateral edge cells, (N,) (operator.py:25-178;
+    the same terms as the boundary diagonals of convdiff.py:204-359): west
+    u- and east outer-face u+ (non-periodic grids only), south v- and north
+    outer-face v+ with the outer-face dx ratio."""
+    nz, ny, nx = g.nz, g.ny, g.nx
+    split = g.split
+    loss = np.zeros((nz, ny, nx))
+    dx3 = np.broadcast_to(g.dx[None, :, None], (nz, ny, nx))
+    if not y_only and not (getattr(g, "periodic_lon", False) and nx > 1):
+        w_out = g.u_minus[:, :, 0] if split else np.maximum(-g.u[:, :, 0], 0.0)
+        loss[:, :, 0] += np.where(w_out > 0, w_out / dx3[:, :, 0], 0.0)
+        e_out = (g.u_plus_e if split else g.u_e)
+        e_cond = e_out > 0 if split else e_out >= 0
+        loss[:, :, -1] += np.where(e_cond, e_out / dx3[:, :, -1], 0.0)
+    if not x_only:
+        dy = g.dy
+        lat_s = g.lat[0] - g.dlat / 2.0
+        lat_n = g.lat[-1] + g.dlat / 2.0
+        tr_s = EARTH_RADIUS * np.cos(lat_s * DEG_TO_RAD) * g.dlon * DEG_TO_RAD / g.dx[0]
+        tr_n = EARTH_RADIUS * np.cos(lat_n * DEG_TO_RAD) * g.dlon * DEG_TO_RAD / g.dx[-1]
+        s_out = g.v_minus[:, 0, :] if split else np.maximum(-g.v[:, 0, :], 0.0)
+        loss[:, 0, :] += np.where(s_out > 0, s_out / dy * tr_s, 0.0)
+        n_out = (g.v_plus_n if split else g.v_n)
+        n_cond = n_out > 0 if split else n_out >= 0
+        loss[:, -1, :] += np.where(n_cond, n_out / dy * tr_n, 0.0)
+    return loss.reshape(-1)
 
 
 def vertical_advection(g):

@@ -4,9 +4,9 @@ TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).  Restates:
 
 * ``vanleer``                        orbit/core/fct.py:38-48
 * ``_vanleer_phi``                   orbit/core/fct.py:235-247
-* ``_horizontal_antidiffusive``      orbit/core/fct.py:256-357 (ghost=None)
+* ``_horizontal_antidiffusive``      orbit/core/fct.py:256-357 (with or without ghost)
 * ``_net_antidiffusive_into_cells``  orbit/core/fct.py:360-378
-* ``_zalesak_2d``                    orbit/core/fct.py:381-447 (ghost=None)
+* ``_zalesak_2d``                    orbit/core/fct.py:381-447 (with or without ghost)
 * ``compute_horizontal_fct_source``  orbit/core/fct.py:459-492
 * ``assemble_fct_linear_operator``   orbit/core/fct.py:495-572
 * the deferred-correction schedule   orbit/cli.py:1204-1241
@@ -30,8 +30,10 @@ def vanleer_phi(c_up, c_far, c_down):
     return vanleer(r)
 
 
-def _faces(g, c):
-    """Anti-diffusive face fluxes and metric weights on x = c/rho."""
+def _faces(g, c, ghost=None):
+    """Anti-diffusive face fluxes and metric weights on x = c/rho; with a ghost
+    field (x-space) its edge-cell values are the far-upwind values beyond the
+    edges and the edge faces keep their reconstruction (fct.py:283-292)."""
     nz, ny, nx = g.nz, g.ny, g.nx
     out = {}
     split = g.split
@@ -40,10 +42,14 @@ def _faces(g, c):
         cL, cR = c[:, :, :-1], c[:, :, 1:]
         cLL = np.concatenate([cL[:, :, :1], c[:, :, :-2]], axis=2)
         cRR = np.concatenate([c[:, :, 2:], cR[:, :, -1:]], axis=2)
+        if ghost is not None:
+            cLL[:, :, 0] = ghost[:, :, 0]
+            cRR[:, :, -1] = ghost[:, :, -1]
         pL = vanleer_phi(cL, cLL, cR)
         pR = vanleer_phi(cR, cRR, cL)
-        pL[:, :, 0] = 0.0
-        pR[:, :, -1] = 0.0
+        if ghost is None:
+            pL[:, :, 0] = 0.0
+            pR[:, :, -1] = 0.0
         up = g.u_plus[:, :, 1:] if split else np.maximum(g.u[:, :, 1:], 0.0)
         um = g.u_minus[:, :, 1:] if split else np.maximum(-g.u[:, :, 1:], 0.0)
         beta = 0.5 * (up * pL + um * pR)
@@ -60,10 +66,14 @@ def _faces(g, c):
         cS, cN = c[:, :-1, :], c[:, 1:, :]
         cSS = np.concatenate([cS[:, :1, :], c[:, :-2, :]], axis=1)
         cNN = np.concatenate([c[:, 2:, :], cN[:, -1:, :]], axis=1)
+        if ghost is not None:
+            cSS[:, 0, :] = ghost[:, 0, :]
+            cNN[:, -1, :] = ghost[:, -1, :]
         pS = vanleer_phi(cS, cSS, cN)
         pN = vanleer_phi(cN, cNN, cS)
-        pS[:, 0, :] = 0.0
-        pN[:, -1, :] = 0.0
+        if ghost is None:
+            pS[:, 0, :] = 0.0
+            pN[:, -1, :] = 0.0
         vp = g.v_plus[:, 1:, :] if split else np.maximum(g.v[:, 1:, :], 0.0)
         vm = g.v_minus[:, 1:, :] if split else np.maximum(-g.v[:, 1:, :], 0.0)
         beta = 0.5 * (vp * pS + vm * pN)
@@ -95,12 +105,13 @@ def _net(g, faces, Cx=None, Cy=None):
     return d
 
 
-def _zalesak(g, c, faces, dt):
+def _zalesak(g, c, faces, dt, ghost=None):
     nz, ny, nx = g.nz, g.ny, g.nx
-    w = np.concatenate([c[:, :, :1], c[:, :, :-1]], axis=2)
-    e = np.concatenate([c[:, :, 1:], c[:, :, -1:]], axis=2)
-    s = np.concatenate([c[:, :1, :], c[:, :-1, :]], axis=1)
-    n = np.concatenate([c[:, 1:, :], c[:, -1:, :]], axis=1)
+    o = c if ghost is None else ghost  # beyond an edge: ghost or clamped
+    w = np.concatenate([o[:, :, :1], c[:, :, :-1]], axis=2)
+    e = np.concatenate([c[:, :, 1:], o[:, :, -1:]], axis=2)
+    s = np.concatenate([o[:, :1, :], c[:, :-1, :]], axis=1)
+    n = np.concatenate([c[:, 1:, :], o[:, -1:, :]], axis=1)
     stk = np.stack([c, w, e, s, n])
     cmax, cmin = stk.max(0), stk.min(0)
     Pp = np.zeros((nz, ny, nx))
@@ -139,13 +150,17 @@ def _zalesak(g, c, faces, dt):
     return Cx, Cy
 
 
-def fct_source(g, c_flat, dt, limited=True):
+def fct_source(g, c_flat, dt, limited=True, c_ghost_flat=None):
     """d_AD = rho * (-div(C (.) A)) on x = c/rho (fct.py:459-492); rho is the
-    state weight, 1 in the pressure form (_state_weights, fct.py:451-456)."""
+    state weight, 1 in the pressure form (_state_weights, fct.py:451-456);
+    ``c_ghost_flat`` the lateral inflow field (fct.py:476-487)."""
     rho = g.state_weights().reshape(-1)
     c = (np.asarray(c_flat, dtype=np.float64) / rho).reshape(g.nz, g.ny, g.nx)
-    faces = _faces(g, c)
-    Cx, Cy = _zalesak(g, c, faces, dt) if limited else (None, None)
+    ghost = None
+    if c_ghost_flat is not None:
+        ghost = (np.asarray(c_ghost_flat, dtype=np.float64) / rho).reshape(g.nz, g.ny, g.nx)
+    faces = _faces(g, c, ghost)
+    Cx, Cy = _zalesak(g, c, faces, dt, ghost) if limited else (None, None)
     return _net(g, faces, Cx, Cy).reshape(-1) * rho
 
 

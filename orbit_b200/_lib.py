@@ -34,7 +34,8 @@ class MetT(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "dP", "Dz", "u", "v", "u_plus", "u_minus", "v_plus", "v_minus", "u_e", "u_plus_e",
         "v_n", "v_plus_n", "kxxyy", "kzz", "w_plus", "w_minus", "cmfmc", "kmu", "kmv", "lat")] + [
-        ("dlat", C.c_double), ("dlon", C.c_double), ("split", C.c_int), ("pressure_form", C.c_int)]
+        ("dlat", C.c_double), ("dlon", C.c_double), ("split", C.c_int), ("pressure_form", C.c_int),
+        ("periodic_lon", C.c_int)] + [(n, C.c_void_p) for n in ("u_wrap", "u_plus_wrap", "u_minus_wrap", "kmu_wrap")]
 
 
 class SpeciesFieldsT(C.Structure):
@@ -60,6 +61,8 @@ EXPORTS = {
     "orbit_symbolic_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "orbit_symbolic_create_ex": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                            C.POINTER(C.c_void_p)]),
+    "orbit_symbolic_create_grid": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, C.POINTER(C.c_void_p)]),
     "orbit_symbolic_destroy": (C.c_int, [C.c_void_p]),
     "orbit_symbolic_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int]),
     "orbit_symbolic_perm": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -67,6 +70,8 @@ EXPORTS = {
                                        C.POINTER(C.c_int64)]),
     "orbit_assemble_transport": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_void_p,
                                            C.c_void_p, C.c_void_p]),
+    "orbit_transport_boundary_loss": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_void_p,
+                                                C.c_void_p]),
     "orbit_mass_balance_rows": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p]),
     "orbit_species_diagonals": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(SpeciesFieldsT), C.c_void_p,
@@ -83,6 +88,10 @@ EXPORTS = {
                                             C.c_void_p, C.c_void_p]),
     "orbit_stencil_apply": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
+    "orbit_fct_source_ghost": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_int, C.c_void_p,
+                                         C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
+    "orbit_stencil_apply_grid": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                           C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_fct_source_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(MetT), C.c_int,
                                            C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_factor_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

@@ -24,8 +24,8 @@ from .synthetic import DTAU, N_BINS, MetBin, SpeciesFields
 
 class OrbitSolver:
     def __init__(self, nz: int, ny: int, nx: int, n_orbits: int, precision: int = 64,
-                 leaf_cells: int = 0, sym: Optional[Symbolic] = None):
-        self.sym = sym if sym is not None else Symbolic(nz, ny, nx, leaf_cells)
+                 leaf_cells: int = 0, sym: Optional[Symbolic] = None, periodic: bool = False):
+        self.sym = sym if sym is not None else Symbolic(nz, ny, nx, leaf_cells, periodic=periodic)
         self.N = self.sym.N
         self.n_orbits = int(n_orbits)
         self.precision = int(precision)

@@ -48,7 +48,7 @@ __device__ __forceinline__ double rho_of(double dP, double Dz) {
 }
 
 __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __restrict__ Tst,
-                           double* __restrict__ rowsum) {
+                           double* __restrict__ rowsum, double* __restrict__ lat_loss) {
   const int64_t NN = (int64_t)nz * ny * nx;
   const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= NN) return;
@@ -66,8 +66,23 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
   auto VM = [&](int64_t c) { return split ? g.v_minus[c] : fmax(-g.v[c], 0.0); };
   const double dPc = g.dP[cell];
   double diag = 0.0, oW = 0.0, oE = 0.0, oS = 0.0, oN = 0.0, oB = 0.0, oT = 0.0;
+  double bloss = 0.0;  // open-outflow terms at the lateral edges (part of diag)
+  const bool px = g.periodic_lon != 0;
+  const int64_t ew = (int64_t)k * ny + j;  // (k, j) index of the wrap-face fields
   // ---- x faces ----
-  if (i > 0) {  // west face: this cell is R
+  if (px && i == 0) {  // wrap face (convdiff.py:150-202): this cell is R, cell nx-1 is L
+    const int64_t L = cell + nx - 1;
+    const double uw = g.u_wrap[ew];
+    const double upw = split ? g.u_plus_wrap[ew] : fmax(uw, 0.0);
+    const double umw = split ? g.u_minus_wrap[ew] : fmax(-uw, 0.0);
+    double rl, rr;
+    face_rates(g.kxxyy[L], g.kxxyy[cell], g.kmu_wrap ? g.kmu_wrap[ew] : 0.0, split, uw, upw, umw, dx, rl, rr);
+    const double dPL = g.dP[L];
+    const bool ok = dPL > 0.0 && dPc > 0.0;
+    const double trR = ok ? 0.5 * (dPL + dPc) / dPc : 1.0;
+    diag += rr * trR;
+    oW = -(rl * trR);
+  } else if (i > 0) {  // west face: this cell is R
     const int64_t L = cell - 1;
     double rl, rr;
     face_rates(g.kxxyy[L], g.kxxyy[cell], g.kmu ? g.kmu[cell] : 0.0, split, g.u[cell], UP(cell),
@@ -79,9 +94,21 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
     oW = -(rl * trR);
   } else {
     const double um = UM(cell);
-    if (um > 0.0) diag += um / dx;
+    if (um > 0.0) bloss += um / dx;
   }
-  if (i < nx - 1) {  // east face: this cell is L
+  if (px && i == nx - 1) {  // wrap face: this cell is L, cell 0 is R
+    const int64_t R = cell - (nx - 1);
+    const double uw = g.u_wrap[ew];
+    const double upw = split ? g.u_plus_wrap[ew] : fmax(uw, 0.0);
+    const double umw = split ? g.u_minus_wrap[ew] : fmax(-uw, 0.0);
+    double rl, rr;
+    face_rates(g.kxxyy[cell], g.kxxyy[R], g.kmu_wrap ? g.kmu_wrap[ew] : 0.0, split, uw, upw, umw, dx, rl, rr);
+    const double dPR = g.dP[R];
+    const bool ok = dPc > 0.0 && dPR > 0.0;
+    const double trL = ok ? 0.5 * (dPc + dPR) / dPc : 1.0;
+    diag += rl * trL;
+    oE = -(rr * trL);
+  } else if (i < nx - 1) {  // east face: this cell is L
     const int64_t R = cell + 1;
     double rl, rr;
     face_rates(g.kxxyy[cell], g.kxxyy[R], g.kmu ? g.kmu[R] : 0.0, split, g.u[R], UP(R), UM(R), dx,
@@ -95,10 +122,10 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
     const int64_t e = (int64_t)k * ny + j;
     if (split) {
       const double up = g.u_plus_e[e];
-      if (up > 0.0) diag += up / dx;
+      if (up > 0.0) bloss += up / dx;
     } else {
       const double ue = g.u_e[e];
-      if (ue >= 0.0) diag += ue / dx;
+      if (ue >= 0.0) bloss += ue / dx;
     }
   }
   // ---- y faces ----
@@ -118,7 +145,7 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
     const double latf = g.lat[0] - g.dlat / 2.0;
     const double tr = dx_at(latf) / dx;
     const double vm = VM(cell);
-    if (vm > 0.0) diag += vm / dy * tr;
+    if (vm > 0.0) bloss += vm / dy * tr;
   }
   if (j < ny - 1) {  // north face: this cell is L (south)
     const int64_t R = cell + nx;
@@ -138,12 +165,17 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
     const int64_t e = (int64_t)k * nx + i;
     if (split) {
       const double vp = g.v_plus_n[e];
-      if (vp > 0.0) diag += vp / dy * tr;
+      if (vp > 0.0) bloss += vp / dy * tr;
     } else {
       const double vn = g.v_n[e];
-      if (vn >= 0.0) diag += vn / dy * tr;
+      if (vn >= 0.0) bloss += vn / dy * tr;
     }
   }
+  if (lat_loss) {
+    lat_loss[cell] = bloss;
+    if (!Tst) return;
+  }
+  diag += bloss;
   // ---- vertical advection (interface k = bottom face, k+1 = top face) ----
   if (dPc > 0.0) {
     if (k >= 1) {
@@ -226,8 +258,8 @@ __global__ void k_assemble(int nz, int ny, int nx, orbit_met_t g, double* __rest
     return (v == 0.0 || g.pressure_form) ? v : rc * v / rho_of(g.dP[nb], g.Dz[nb]);
   };
   Tst[0 * NN + cell] = diag;
-  Tst[1 * NN + cell] = i > 0 ? sim(oW, cell - 1) : 0.0;
-  Tst[2 * NN + cell] = i < nx - 1 ? sim(oE, cell + 1) : 0.0;
+  Tst[1 * NN + cell] = i > 0 ? sim(oW, cell - 1) : px ? sim(oW, cell + nx - 1) : 0.0;
+  Tst[2 * NN + cell] = i < nx - 1 ? sim(oE, cell + 1) : px ? sim(oE, cell - (nx - 1)) : 0.0;
   Tst[3 * NN + cell] = j > 0 ? sim(oS, cell - nx) : 0.0;
   Tst[4 * NN + cell] = j < ny - 1 ? sim(oN, cell + nx) : 0.0;
   Tst[5 * NN + cell] = k > 0 ? sim(oB, cell - nxy) : 0.0;
@@ -270,7 +302,7 @@ __global__ void k_mass_rows(int nz, int ny, int nx, const double* const* Tst, co
 // y_v = beta y_v + alpha S_v x_v (or S_v^T x_v) for 7-point stencils S_v
 // ([7][N]: centre, W, E, S, N, below, above; entries pointing outside the
 // grid are ignored) and vectors x_v, one (vector, cell) per thread.
-__global__ void k_stencil_apply(int nz, int ny, int nx, const double* __restrict__ S_all,
+__global__ void k_stencil_apply(int nz, int ny, int nx, int px, const double* __restrict__ S_all,
                                 const double* __restrict__ x_all, double alpha, double beta, int trans,
                                 double* __restrict__ y_all) {
   const int64_t N = (int64_t)nz * ny * nx;
@@ -279,41 +311,42 @@ __global__ void k_stencil_apply(int nz, int ny, int nx, const double* __restrict
   const double* S = S_all + (int64_t)blockIdx.y * 7 * N;
   const double* x = x_all + (int64_t)blockIdx.y * N;
   double* y = y_all + (int64_t)blockIdx.y * N;
-  const int i = (int)(p % nx), j = (int)((p / nx) % ny), k = (int)(p / ((int64_t)nx * ny));
-  const int64_t off[7] = {0, -1, 1, -(int64_t)nx, (int64_t)nx, -(int64_t)nx * ny, (int64_t)nx * ny};
-  const bool ok[7] = {true, i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
-  double acc = 0.0;
+  int64_t nb[6];
+  bool has[6];
+  stencil_nbrs(p, nz, ny, nx, px, nb, has);
+  double acc = S[p] * x[p];
   if (!trans) {
 #pragma unroll
-    for (int d = 0; d < 7; ++d)
-      if (ok[d]) acc += S[d * N + p] * x[p + off[d]];
+    for (int d = 0; d < 6; ++d)
+      if (has[d]) acc += S[(d + 1) * N + p] * x[nb[d]];
   } else {
-    // (S^T x)_p = sum over the rows q = p - off[d] whose entry d points at p
-    const bool okt[7] = {true, i < nx - 1, i > 0, j < ny - 1, j > 0, k < nz - 1, k > 0};
+    // (S^T x)_p = sum over the neighbours q of their entries pointing at p
+    // (the opposite direction: W <-> E, S <-> N, B <-> T)
+    const int opp[6] = {2, 1, 4, 3, 6, 5};
 #pragma unroll
-    for (int d = 0; d < 7; ++d)
-      if (okt[d]) acc += S[d * N + p - off[d]] * x[p - off[d]];
+    for (int d = 0; d < 6; ++d)
+      if (has[d]) acc += S[opp[d] * N + nb[d]] * x[nb[d]];
   }
   y[p] = (beta != 0.0 ? beta * y[p] : 0.0) + alpha * acc;
 }
 
 }  // namespace
 
-int stencil_apply(int nz, int ny, int nx, int n_vec, const double* S, const double* x, double alpha, double beta,
-                  int trans, double* y, cudaStream_t st) {
+int stencil_apply(int nz, int ny, int nx, int px, int n_vec, const double* S, const double* x, double alpha,
+                  double beta, int trans, double* y, cudaStream_t st) {
   const int64_t N = (int64_t)nz * ny * nx;
   dim3 g((unsigned)((N + 255) / 256), n_vec);
-  k_stencil_apply<<<g, 256, 0, st>>>(nz, ny, nx, S, x, alpha, beta, trans, y);
+  k_stencil_apply<<<g, 256, 0, st>>>(nz, ny, nx, px, S, x, alpha, beta, trans, y);
   note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;
 }
 
 int assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T, double* rowsum,
-                       cudaStream_t st) {
+                       double* lat_loss, cudaStream_t st) {
   const int64_t NN = (int64_t)nz * ny * nx;
   const int threads = 128;
-  k_assemble<<<(unsigned)((NN + threads - 1) / threads), threads, 0, st>>>(nz, ny, nx, *met, T, rowsum);
+  k_assemble<<<(unsigned)((NN + threads - 1) / threads), threads, 0, st>>>(nz, ny, nx, *met, T, rowsum, lat_loss);
   note_launch();
   ORBIT_CUDA_TRY(cudaGetLastError());
   return ORBIT_OK;

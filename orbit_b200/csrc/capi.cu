@@ -47,18 +47,18 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
 int chain_apply_impl(orbit_factor_s* f, int n, int trans, int tau0, int tau1, const double* x_in,
                      double* x_out, const double* forcing, double fscale, int refine, cudaStream_t st);
 int assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, double* T, double* rowsum,
-                       cudaStream_t st);
+                       double* lat_loss, cudaStream_t st);
 int chain_wait_selftest(orbit_factor_s* f, const int* d_orbit_ids, cudaStream_t st);
 int mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* Tst,
                       const double* const* rho, double* out_int, double* out_top, cudaStream_t st);
 int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
-               int limited, double* d, double* scratch, cudaStream_t st);
+               int limited, double* d, double* scratch, cudaStream_t st, const double* ghost = nullptr);
 int fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
                        double dt, int limited, double* d, cudaStream_t st);
 int fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
                         double* stencil, double* scratch, cudaStream_t st);
-int stencil_apply(int nz, int ny, int nx, int n_vec, const double* S, const double* x, double alpha, double beta,
-                  int trans, double* y, cudaStream_t st);
+int stencil_apply(int nz, int ny, int nx, int px, int n_vec, const double* S, const double* x, double alpha,
+                  double beta, int trans, double* y, cudaStream_t st);
 
 namespace {
 
@@ -211,6 +211,11 @@ int orbit_factor_profile(orbit_factor_t f, int mode, double* out) {
 
 int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_elems, int tc_min_n,
                              int subtree_div, orbit_symbolic_t* out) {
+  return orbit_symbolic_create_grid(nz, ny, nx, 0, leaf_cells, chunk_elems, tc_min_n, subtree_div, out);
+}
+
+int orbit_symbolic_create_grid(int nz, int ny, int nx, int periodic_x, int leaf_cells, int chunk_elems,
+                               int tc_min_n, int subtree_div, orbit_symbolic_t* out) {
   if (!out) {
     set_last_error("out is NULL");
     return ORBIT_ERR_ARG;
@@ -228,6 +233,7 @@ int orbit_symbolic_create_ex(int nz, int ny, int nx, int leaf_cells, int chunk_e
   opt.tc_min_n = std::max(1, tc_min_n > 0 ? tc_min_n : env_int("ORBIT_B200_TC_MIN_N", opt.tc_min_n));
   opt.subtree_div = subtree_div >= 0 ? subtree_div : std::max(0, env_int("ORBIT_B200_SUBTREE_DIV", 0));
   opt.fuse_max_n = std::max(0, env_int("ORBIT_B200_FUSED_MAX_N", kFrontMaxN));
+  opt.periodic_x = periodic_x ? 1 : 0;
   orbit_symbolic_s* h = new (std::nothrow) orbit_symbolic_s();
   if (!h) return ORBIT_ERR_NOMEM;
   std::string err = build_symbolic(nz, ny, nx, opt, h->S);
@@ -338,7 +344,27 @@ int orbit_assemble_transport(int nz, int ny, int nx, const orbit_met_t* met, dou
     set_last_error("orbit_assemble_transport: missing meteorology field");
     return ORBIT_ERR_ARG;
   }
-  return assemble_transport(nz, ny, nx, met, T_stencil, rowsum, (cudaStream_t)stream);
+  if (met->periodic_lon && (nx < 3 || !met->u_wrap || (met->split && (!met->u_plus_wrap || !met->u_minus_wrap)))) {
+    set_last_error("orbit_assemble_transport: a periodic-longitude grid needs nx >= 3 and the wrap-face fields");
+    return ORBIT_ERR_ARG;
+  }
+  return assemble_transport(nz, ny, nx, met, T_stencil, rowsum, nullptr, (cudaStream_t)stream);
+}
+
+int orbit_transport_boundary_loss(int nz, int ny, int nx, const orbit_met_t* met, double* loss,
+                                  orbit_stream_t stream) {
+  if (!met || !loss || nz < 1 || ny < 2 || nx < 2) {
+    set_last_error("orbit_transport_boundary_loss: bad arguments (need nz>=1, ny>=2, nx>=2)");
+    return ORBIT_ERR_ARG;
+  }
+  if (!met->dP || !met->Dz || !met->u || !met->v || !met->kxxyy || !met->kzz || !met->w_plus ||
+      !met->w_minus || !met->lat || (met->split && (!met->u_minus || !met->v_minus || !met->u_plus_e ||
+                                                    !met->v_plus_n)) ||
+      (!met->split && (!met->u_e || !met->v_n))) {
+    set_last_error("orbit_transport_boundary_loss: missing meteorology field");
+    return ORBIT_ERR_ARG;
+  }
+  return assemble_transport(nz, ny, nx, met, nullptr, nullptr, loss, (cudaStream_t)stream);
 }
 
 int orbit_mass_balance_rows(int nz, int ny, int nx, int nbins, const double* const* T_stencils,
@@ -389,13 +415,39 @@ int orbit_fct_linear_operator(int nz, int ny, int nx, const orbit_met_t* met, in
   return rc;
 }
 
+int orbit_fct_source_ghost(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,
+                           const double* c_ghost, double dt, int limited, double* d, orbit_stream_t stream) {
+  if (!met || !c || !c_ghost || !d || n_vec < 1 || nz < 1 || ny < 1 || nx < 1 || !(dt > 0)) {
+    set_last_error("orbit_fct_source_ghost: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t N = (int64_t)nz * ny * nx;
+  double* scratch = nullptr;
+  ORBIT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(double) * 3 * N * n_vec, st));
+  int rc = fct_source(nz, ny, nx, met, n_vec, c, dt, limited, d, scratch, st, c_ghost);
+  cudaFreeAsync(scratch, st);
+  return rc;
+}
+
 int orbit_stencil_apply(int nz, int ny, int nx, int n_vec, const double* stencils, const double* x, double alpha,
                         double beta, int trans, double* y, orbit_stream_t stream) {
   if (!stencils || !x || !y || n_vec < 1 || nz < 1 || ny < 1 || nx < 1) {
     set_last_error("orbit_stencil_apply: bad arguments");
     return ORBIT_ERR_ARG;
   }
-  return stencil_apply(nz, ny, nx, n_vec, stencils, x, alpha, beta, trans, y, (cudaStream_t)stream);
+  return stencil_apply(nz, ny, nx, 0, n_vec, stencils, x, alpha, beta, trans, y, (cudaStream_t)stream);
+}
+
+int orbit_stencil_apply_grid(int nz, int ny, int nx, int periodic_x, int n_vec, const double* stencils,
+                             const double* x, double alpha, double beta, int trans, double* y,
+                             orbit_stream_t stream) {
+  if (!stencils || !x || !y || n_vec < 1 || nz < 1 || ny < 1 || nx < 1 || (periodic_x && nx < 3)) {
+    set_last_error("orbit_stencil_apply_grid: bad arguments");
+    return ORBIT_ERR_ARG;
+  }
+  return stencil_apply(nz, ny, nx, periodic_x ? 1 : 0, n_vec, stencils, x, alpha, beta, trans, y,
+                       (cudaStream_t)stream);
 }
 
 int orbit_fct_source_noalloc(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c,

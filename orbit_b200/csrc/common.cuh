@@ -25,6 +25,29 @@ int allow_max_smem(const void* func);
     }                                                                            \
   } while (0)
 
+// Neighbours of cell c of an (nz, ny, nx) grid in the stencil order W E S N
+// B T, and whether each exists.  With px set (periodic longitude, nx >= 3)
+// the x neighbours of the first and last columns wrap around: the stencil's
+// W entry of a cell with i = 0 couples it to i = nx - 1 and the E entry of
+// i = nx - 1 to i = 0 (orbit/core/convdiff.py:150-202).
+__device__ __forceinline__ void stencil_nbrs(int64_t c, int nz, int ny, int nx, int px, int64_t nb[6],
+                                             bool has[6]) {
+  const int64_t nxy = (int64_t)nx * ny;
+  const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  nb[0] = i > 0 ? c - 1 : c + nx - 1;
+  nb[1] = i < nx - 1 ? c + 1 : c - (nx - 1);
+  nb[2] = c - nx;
+  nb[3] = c + nx;
+  nb[4] = c - nxy;
+  nb[5] = c + nxy;
+  has[0] = i > 0 || px;
+  has[1] = i < nx - 1 || px;
+  has[2] = j > 0;
+  has[3] = j < ny - 1;
+  has[4] = k > 0;
+  has[5] = k < nz - 1;
+}
+
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
   asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

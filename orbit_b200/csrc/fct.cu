@@ -2,7 +2,8 @@
 //
 // Replaces compute_horizontal_fct_source (orbit/core/fct.py:459-492) with its
 // helpers _vanleer_phi (fct.py:235-247), _horizontal_antidiffusive
-// (fct.py:256-357, no ghost cells), _zalesak_2d (fct.py:381-447) and
+// (fct.py:256-357, with or without the lateral-inflow ghost field),
+// _zalesak_2d (fct.py:381-447) and
 // _net_antidiffusive_into_cells (fct.py:360-378).  Pass 1 computes, per cell,
 // the Zalesak ratios R+/R- from the four face fluxes touching it and the
 // 5-point bounds; pass 2 limits every face with the ratios of its two cells
@@ -24,7 +25,11 @@ struct FctGeom {
   orbit_met_t g;
   int nz, ny, nx;
   double dt;
+  // optional lateral-inflow concentration per vector (c-space, same layout as
+  // c): its edge-cell values stand for the cells beyond each lateral edge
+  const double* ghost = nullptr;
 };
+
 
 // State weight of a cell: rho = dP / (g Dz) in the concentration form, 1 in the
 // pressure form (_state_weights, fct.py:451-456).
@@ -32,6 +37,11 @@ __device__ __forceinline__ double rho_at(const orbit_met_t& g, int64_t c) {
   if (g.pressure_form) return 1.0;
   const double dP = g.dP[c], Dz = g.Dz[c];
   return (dP > 0.0 && Dz > 0.0) ? dP / (kGravity * Dz) : 1.0;
+}
+
+// Value beyond the edge at edge cell e, in x = c / rho.
+__device__ __forceinline__ double ghost_x(const orbit_met_t& g, const double* gh, int64_t e) {
+  return gh[e] / rho_at(g, e);
 }
 
 __device__ __forceinline__ double vl_phi(double up, double far, double down) {
@@ -54,18 +64,21 @@ struct Face {
   bool ok;
 };
 
-__device__ Face x_face(const FctGeom& G, const double* x, int k, int j, int ihi) {
+// gh: the ghost field of this vector or null (fct.py:283-292: with a ghost
+// field the far-upwind value beyond an edge is the ghost value of the edge
+// cell; without one the face drops to first order there).
+__device__ Face x_face(const FctGeom& G, const double* x, int k, int j, int ihi, const double* gh) {
   const orbit_met_t& g = G.g;
   const int nx = G.nx;
   const int64_t base = ((int64_t)k * G.ny + j) * nx;
   const int64_t hi = base + ihi, lo = hi - 1;
   const double cL = x[lo], cR = x[hi];
-  const double cLL = ihi - 1 > 0 ? x[lo - 1] : cL;
-  const double cRR = ihi < nx - 1 ? x[hi + 1] : cR;
+  const double cLL = ihi - 1 > 0 ? x[lo - 1] : gh ? ghost_x(g, gh, lo) : cL;
+  const double cRR = ihi < nx - 1 ? x[hi + 1] : gh ? ghost_x(g, gh, hi) : cR;
   double pL = vl_phi(cL, cLL, cR);
   double pR = vl_phi(cR, cRR, cL);
-  if (ihi - 1 == 0) pL = 0.0;
-  if (ihi == nx - 1) pR = 0.0;
+  if (!gh && ihi - 1 == 0) pL = 0.0;
+  if (!gh && ihi == nx - 1) pR = 0.0;
   const double up = G.g.split ? g.u_plus[hi] : fmax(g.u[hi], 0.0);
   const double um = G.g.split ? g.u_minus[hi] : fmax(-g.u[hi], 0.0);
   const double beta = 0.5 * (up * pL + um * pR);
@@ -84,17 +97,17 @@ __device__ Face x_face(const FctGeom& G, const double* x, int k, int j, int ihi)
   return f;
 }
 
-__device__ Face y_face(const FctGeom& G, const double* x, int k, int jhi, int i) {
+__device__ Face y_face(const FctGeom& G, const double* x, int k, int jhi, int i, const double* gh) {
   const orbit_met_t& g = G.g;
   const int nx = G.nx, ny = G.ny;
   const int64_t hi = ((int64_t)k * ny + jhi) * nx + i, lo = hi - nx;
   const double cS = x[lo], cN = x[hi];
-  const double cSS = jhi - 1 > 0 ? x[lo - nx] : cS;
-  const double cNN = jhi < ny - 1 ? x[hi + nx] : cN;
+  const double cSS = jhi - 1 > 0 ? x[lo - nx] : gh ? ghost_x(g, gh, lo) : cS;
+  const double cNN = jhi < ny - 1 ? x[hi + nx] : gh ? ghost_x(g, gh, hi) : cN;
   double pS = vl_phi(cS, cSS, cN);
   double pN = vl_phi(cN, cNN, cS);
-  if (jhi - 1 == 0) pS = 0.0;
-  if (jhi == ny - 1) pN = 0.0;
+  if (!gh && jhi - 1 == 0) pS = 0.0;
+  if (!gh && jhi == ny - 1) pN = 0.0;
   const double vp = G.g.split ? g.v_plus[hi] : fmax(g.v[hi], 0.0);
   const double vm = G.g.split ? g.v_minus[hi] : fmax(-g.v[hi], 0.0);
   const double beta = 0.5 * (vp * pS + vm * pN);
@@ -127,12 +140,15 @@ __global__ void k_fct_ratio(FctGeom G, const double* x_all, double* Rp_all, doub
   const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= N) return;
   const double* x = x_all + (int64_t)blockIdx.y * N;
+  const double* gh = G.ghost ? G.ghost + (int64_t)blockIdx.y * N : nullptr;
   const int nx = G.nx, ny = G.ny;
   const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
   const double c = x[cell];
   double cmax = c, cmin = c;
-  const double w = i > 0 ? x[cell - 1] : c, e = i < nx - 1 ? x[cell + 1] : c;
-  const double s = j > 0 ? x[cell - nx] : c, n = j < ny - 1 ? x[cell + nx] : c;
+  // beyond an edge: the edge cell's ghost value, or the cell itself (clamped)
+  const double out = gh ? ghost_x(G.g, gh, cell) : c;
+  const double w = i > 0 ? x[cell - 1] : out, e = i < nx - 1 ? x[cell + 1] : out;
+  const double s = j > 0 ? x[cell - nx] : out, n = j < ny - 1 ? x[cell + nx] : out;
   cmax = fmax(fmax(fmax(cmax, w), fmax(e, s)), n);
   cmin = fmin(fmin(fmin(cmin, w), fmin(e, s)), n);
   double Pp = 0.0, Pm = 0.0;
@@ -142,21 +158,21 @@ __global__ void k_fct_ratio(FctGeom G, const double* x_all, double* Rp_all, doub
   };
   if (nx > 1) {
     if (i > 0) {
-      Face f = x_face(G, x, k, j, i);
+      Face f = x_face(G, x, k, j, i, gh);
       acc(f.ok ? f.trR * f.flux : 0.0);
     }
     if (i < nx - 1) {
-      Face f = x_face(G, x, k, j, i + 1);
+      Face f = x_face(G, x, k, j, i + 1, gh);
       acc(f.ok ? -f.trL * f.flux : 0.0);
     }
   }
   if (ny > 1) {
     if (j > 0) {
-      Face f = y_face(G, x, k, j, i);
+      Face f = y_face(G, x, k, j, i, gh);
       acc(f.ok ? f.trR * f.flux : 0.0);
     }
     if (j < ny - 1) {
-      Face f = y_face(G, x, k, j + 1, i);
+      Face f = y_face(G, x, k, j + 1, i, gh);
       acc(f.ok ? -f.trL * f.flux : 0.0);
     }
   }
@@ -172,6 +188,7 @@ __global__ void k_fct_div(FctGeom G, const double* x_all, const double* Rp_all, 
   const double* x = x_all + (int64_t)blockIdx.y * N;
   const double* Rp = Rp_all + (int64_t)blockIdx.y * N;
   const double* Rm = Rm_all + (int64_t)blockIdx.y * N;
+  const double* gh = G.ghost ? G.ghost + (int64_t)blockIdx.y * N : nullptr;
   const int nx = G.nx, ny = G.ny;
   const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
   auto limiter = [&](const Face& f, int64_t lo, int64_t hi) {
@@ -183,24 +200,24 @@ __global__ void k_fct_div(FctGeom G, const double* x_all, const double* Rp_all, 
   double d = 0.0;
   if (nx > 1) {
     if (i > 0) {
-      Face f = x_face(G, x, k, j, i);
+      Face f = x_face(G, x, k, j, i, gh);
       const double fl = limiter(f, cell - 1, cell) * f.flux;
       d += f.ok ? f.trR * fl : 0.0;
     }
     if (i < nx - 1) {
-      Face f = x_face(G, x, k, j, i + 1);
+      Face f = x_face(G, x, k, j, i + 1, gh);
       const double fl = limiter(f, cell, cell + 1) * f.flux;
       d -= f.ok ? f.trL * fl : 0.0;
     }
   }
   if (ny > 1) {
     if (j > 0) {
-      Face f = y_face(G, x, k, j, i);
+      Face f = y_face(G, x, k, j, i, gh);
       const double fl = limiter(f, cell - nx, cell) * f.flux;
       d += f.ok ? f.trR * fl : 0.0;
     }
     if (j < ny - 1) {
-      Face f = y_face(G, x, k, j + 1, i);
+      Face f = y_face(G, x, k, j + 1, i, gh);
       const double fl = limiter(f, cell, cell + nx) * f.flux;
       d -= f.ok ? f.trL * fl : 0.0;
     }
@@ -223,6 +240,7 @@ __global__ void k_fct_linop(FctGeom G, const double* x_all, const double* Rp_all
   const double* Rp = Rp_all + (int64_t)blockIdx.y * N;
   const double* Rm = Rm_all + (int64_t)blockIdx.y * N;
   double* st = st_all + (int64_t)blockIdx.y * 7 * N;
+  const double* gh = nullptr;  // the frozen operator has no ghost field (fct.py:495-572)
   const int nx = G.nx, ny = G.ny;
   const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
   auto gain = [&](const Face& f, int64_t lo, int64_t hi) {
@@ -235,13 +253,13 @@ __global__ void k_fct_linop(FctGeom G, const double* x_all, const double* Rp_all
   double cen = 0.0, w = 0.0, e = 0.0, s = 0.0, n = 0.0;
   if (nx > 1) {
     if (i > 0) {  // west face: this cell is its high side
-      const Face f = x_face(G, x, k, j, i);
+      const Face f = x_face(G, x, k, j, i, gh);
       const double wr = f.trR * gain(f, cell - 1, cell);
       cen -= wr;
       w = wr * rp / rho_at(G.g, cell - 1);
     }
     if (i < nx - 1) {  // east face: low side
-      const Face f = x_face(G, x, k, j, i + 1);
+      const Face f = x_face(G, x, k, j, i + 1, gh);
       const double wl = f.trL * gain(f, cell, cell + 1);
       cen -= wl;
       e = wl * rp / rho_at(G.g, cell + 1);
@@ -249,13 +267,13 @@ __global__ void k_fct_linop(FctGeom G, const double* x_all, const double* Rp_all
   }
   if (ny > 1) {
     if (j > 0) {
-      const Face f = y_face(G, x, k, j, i);
+      const Face f = y_face(G, x, k, j, i, gh);
       const double wr = f.trR * gain(f, cell - nx, cell);
       cen -= wr;
       s = wr * rp / rho_at(G.g, cell - nx);
     }
     if (j < ny - 1) {
-      const Face f = y_face(G, x, k, j + 1, i);
+      const Face f = y_face(G, x, k, j + 1, i, gh);
       const double wl = f.trL * gain(f, cell, cell + nx);
       cen -= wl;
       n = wl * rp / rho_at(G.g, cell + nx);
@@ -273,9 +291,9 @@ __global__ void k_fct_linop(FctGeom G, const double* x_all, const double* Rp_all
 }  // namespace
 
 int fct_source(int nz, int ny, int nx, const orbit_met_t* met, int n_vec, const double* c, double dt,
-               int limited, double* d, double* scratch, cudaStream_t st) {
+               int limited, double* d, double* scratch, cudaStream_t st, const double* ghost = nullptr) {
   const int64_t N = (int64_t)nz * ny * nx;
-  FctGeom G{*met, nz, ny, nx, dt};
+  FctGeom G{*met, nz, ny, nx, dt, ghost};
   double* x = scratch;
   double* Rp = scratch + (int64_t)n_vec * N;
   double* Rm = Rp + (int64_t)n_vec * N;

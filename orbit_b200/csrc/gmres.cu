@@ -241,7 +241,7 @@ __global__ void k_init_g(double* g, double* scal, const int* ids, int B) {
 // r = b - A x on the permuted 7-point stencil (FP64), trans: r = b - A^T x
 __global__ void k_stencil_resid(double* r, int64_t rs, const double* b, int64_t bs, const double* x,
                                 int64_t xs, const double* Ast, int tau, const int32_t* perm,
-                                const int32_t* iperm, int nz, int ny, int nx, int trans, const int* ids,
+                                const int32_t* iperm, int nz, int ny, int nx, int px, int trans, const int* ids,
                                 const int* set_of, int n_bins) {
   const int o = ids[blockIdx.y];
   const int64_t N = (int64_t)nz * ny * nx;
@@ -249,14 +249,13 @@ __global__ void k_stencil_resid(double* r, int64_t rs, const double* b, int64_t 
   const double* xv = x + (int64_t)o * xs;
   const double* bv = b + (int64_t)o * bs;
   double* rv = r + (int64_t)o * rs;
-  const int64_t nxy = (int64_t)nx * ny;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = perm[p];
-    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
     double acc = A[c] * xv[p];
     // neighbours: W E S N B T, opposite directions E W N S T B
-    const int64_t nb[6] = {c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy};
-    const bool has[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+    int64_t nb[6];
+    bool has[6];
+    stencil_nbrs(c, nz, ny, nx, px, nb, has);
     const int opp[6] = {2, 1, 4, 3, 6, 5};
 #pragma unroll
     for (int d = 0; d < 6; ++d) {
@@ -272,17 +271,16 @@ __global__ void k_stencil_resid(double* r, int64_t rs, const double* b, int64_t 
 // (c_0 := c_8):  R_tau = fs e_tau + c_tau - A_tau c_{tau+1}, FP64, permuted order.
 // C: per orbit 9 vectors (slot 0 unused, c_0 read from slot 8); E, R: per orbit 8 vectors.
 __global__ void k_block_resid(double* R, const double* E, double fs, const double* Cb, const double* Ast,
-                              const int32_t* perm, const int32_t* iperm, int nz, int ny, int nx,
+                              const int32_t* perm, const int32_t* iperm, int nz, int ny, int nx, int px,
                               const int* ids, const int* set_of) {
   const int o = ids[blockIdx.y];
   const int64_t N = (int64_t)nz * ny * nx;
-  const int64_t nxy = (int64_t)nx * ny;
   const double* C = Cb + (int64_t)o * 9 * N;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = perm[p];
-    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
-    const int64_t nb[6] = {c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy};
-    const bool has[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+    int64_t nb[6];
+    bool has[6];
+    stencil_nbrs(c, nz, ny, nx, px, nb, has);
     int64_t q[6];
 #pragma unroll
     for (int d = 0; d < 6; ++d) q[d] = has[d] ? iperm[nb[d]] : 0;
@@ -309,18 +307,17 @@ __global__ void k_block_resid(double* R, const double* E, double fs, const doubl
 // R: per orbit 8 receptors.
 __global__ void k_block_resid_T(double* Rs, double* rho7, int64_t r7s, const double* R, const double* Lb,
                                 const double* Ast, const int32_t* perm, const int32_t* iperm, int nz, int ny,
-                                int nx, const int* ids, const int* set_of) {
+                                int nx, int px, const int* ids, const int* set_of) {
   const int o = ids[blockIdx.y];
   const int64_t N = (int64_t)nz * ny * nx;
-  const int64_t nxy = (int64_t)nx * ny;
   const double* L = Lb + (int64_t)o * 9 * N;
   const double* Ro = R + (int64_t)o * 8 * N;
   double* Ro_s = Rs + (int64_t)o * 8 * N;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = perm[p];
-    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
-    const int64_t nb[6] = {c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy};
-    const bool has[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+    int64_t nb[6];
+    bool has[6];
+    stencil_nbrs(c, nz, ny, nx, px, nb, has);
     const int opp[6] = {2, 1, 4, 3, 6, 5};
     int64_t q[6];
 #pragma unroll
@@ -445,7 +442,7 @@ int refined_bin(Ctx& c, const int* d_ids, int B, int tau, int tau1, const double
   k_lincomb<<<g, kVT, 0, c.st>>>(c.Tv, c.vs, one, XS + bin_out * N, xs, one, nullptr, 0, d_ids, N);
   note_launch();
   k_stencil_resid<<<g, kVT, 0, c.st>>>(c.Rv, c.vs, XS + bin_in * N, xs, c.Tv, c.vs, f->A_stencil, tau,
-                                       sy->d.perm, sy->d.iperm, sy->S.nz, sy->S.ny, sy->S.nx, trans, d_ids,
+                                       sy->d.perm, sy->d.iperm, sy->S.nz, sy->S.ny, sy->S.nx, sy->S.periodic_x, trans, d_ids,
                                        f->set_of, f->n_bins);
   note_launch();
   k_lincomb<<<g, kVT, 0, c.st>>>(XS + bin_in * N, xs, one, c.Rv, c.vs, one, nullptr, 0, d_ids, N);
@@ -771,7 +768,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
       if (rc) return rc;
       const dim3 gb = vgrid(N, B);
       k_block_resid<<<gb, kVT, 0, st>>>(Rb, f->E, dtau, Cb, f->A_stencil, sy->d.perm, sy->d.iperm, sy->S.nz,
-                                        sy->S.ny, sy->S.nx, d_ids, f->set_of);
+                                        sy->S.ny, sy->S.nx, sy->S.periodic_x, d_ids, f->set_of);
       note_launch();
       if (it == 0 && !warm) {
         // from c = 0 the residual forcing is dtau e itself, whose sweep is the
@@ -882,7 +879,7 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
       if (rc) return rc;
       const dim3 gb = vgrid(N, B);
       k_block_resid_T<<<gb, kVT, 0, st>>>(Rs, rho7, c.vs, f->E, Lb, f->A_stencil, sy->d.perm, sy->d.iperm, sy->S.nz,
-                                          sy->S.ny, sy->S.nx, d_ids, f->set_of);
+                                          sy->S.ny, sy->S.nx, sy->S.periodic_x, d_ids, f->set_of);
       note_launch();
       // s_rho: transposed sweep from X[8] = rho_7 with the shifted forcing
       ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));

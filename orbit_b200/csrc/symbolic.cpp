@@ -10,7 +10,10 @@
 // its unknowns are eliminated after both half-boxes, and after elimination it
 // is coupled densely to exactly the cells of ancestor planes that touch its box
 // (the 6-neighbours of the box), which gives the multifrontal update sets
-// without any graph search.
+// without any graph search.  On a periodic-longitude grid a box that spans
+// every column is a ring: cut across x it needs two planes (its first column
+// and its middle column), which leave two ordinary boxes; the x-neighbours of
+// a box touching column 0 or nx - 1 wrap around.
 #include "symbolic.h"
 
 #include <algorithm>
@@ -34,6 +37,9 @@ struct Box {
 struct Node {
   Box box;      // region of the subtree
   Box own;      // own cells (separator plane or the leaf box)
+  Box own2;     // second separator plane of a ring cut across x (when two)
+  bool two = false;
+  bool ring = false;  // spans every column of a periodic grid
   int c[2] = {-1, -1};
   int parent = -1;
   int depth = 0;
@@ -45,11 +51,14 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
   int leaf_cells = opt.leaf_cells;
   int chunk_elems = opt.chunk_elems;
   if (nz < 1 || ny < 1 || nx < 1) return "grid dimensions must be positive";
+  if (opt.periodic_x && nx < 3) return "a periodic-longitude grid needs at least 3 columns";
   if (int64_t(nz) * ny * nx > (int64_t(1) << 30)) return "grid too large";
   if (leaf_cells < 1) leaf_cells = 1;
   if (chunk_elems < 256) chunk_elems = 256;
   S = Symbolic();
   S.nz = nz; S.ny = ny; S.nx = nx;
+  S.periodic_x = opt.periodic_x ? 1 : 0;
+  const bool px = S.periodic_x != 0;
   S.N = int64_t(nz) * ny * nx;
   S.leaf_cells = leaf_cells;
   const int64_t N = S.N;
@@ -57,11 +66,12 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
 
   // ---- recursive dissection (explicit stack, postorder numbering) ----
   std::vector<Node> nodes;
-  std::function<int(const Box&, int, int)> rec = [&](const Box& b, int depth, int par) -> int {
+  std::function<int(const Box&, int, int, bool)> rec = [&](const Box& b, int depth, int par, bool ring) -> int {
     Node nd;
     nd.box = b;
     nd.depth = depth;
     nd.parent = par;
+    nd.ring = ring;
     int ext[3] = {b.hi[0] - b.lo[0], b.hi[1] - b.lo[1], b.hi[2] - b.lo[2]};
     int kids[2] = {-1, -1};
     if (b.cells() <= leaf_cells || (ext[0] <= 1 && ext[1] <= 1 && ext[2] <= 1)) {
@@ -75,15 +85,24 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
       Box sep = b; sep.lo[a] = mid; sep.hi[a] = mid + 1;
       Box c1 = b; c1.hi[a] = mid;
       Box c2 = b; c2.lo[a] = mid + 1;
-      nd.own = sep;
+      bool kid_ring = ring;
+      if (ring && a == 2) {
+        // ring cut across x: planes at its first and middle columns
+        Box sep0 = b; sep0.lo[2] = b.lo[2]; sep0.hi[2] = b.lo[2] + 1;
+        nd.own = sep0;
+        nd.own2 = sep;
+        nd.two = true;
+        c1.lo[2] = b.lo[2] + 1;
+        kid_ring = false;
+      } else {
+        nd.own = sep;
+      }
       int slot = 0;
       // children first (postorder), recorded after the recursion
-      int self_placeholder = -1;
-      (void)self_placeholder;
       std::vector<Box> cb;
       if (c1.hi[a] > c1.lo[a]) cb.push_back(c1);
       if (c2.hi[a] > c2.lo[a]) cb.push_back(c2);
-      for (auto& cbx : cb) kids[slot++] = rec(cbx, depth + 1, -2);
+      for (auto& cbx : cb) kids[slot++] = rec(cbx, depth + 1, -2, kid_ring);
     }
     nd.c[0] = kids[0];
     nd.c[1] = kids[1];
@@ -94,7 +113,7 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
     return id;
   };
   Box root{{0, 0, 0}, {nz, ny, nx}};
-  rec(root, 0, -1);
+  rec(root, 0, -1, px);
   const int ns = int(nodes.size());
   S.nsuper = ns;
 
@@ -107,15 +126,17 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
   for (int s = 0; s < ns; ++s) {
     const Node& nd = nodes[s];
     S.first[s] = int32_t(next);
-    const Box& o = nd.own;
-    for (int k = o.lo[0]; k < o.hi[0]; ++k)
-      for (int j = o.lo[1]; j < o.hi[1]; ++j)
-        for (int i = o.lo[2]; i < o.hi[2]; ++i) {
-          int64_t cell = (int64_t(k) * ny + j) * nx + i;
-          S.perm[next] = int32_t(cell);
-          S.iperm[cell] = int32_t(next);
-          ++next;
-        }
+    for (int q = 0; q < (nd.two ? 2 : 1); ++q) {
+      const Box& o = q ? nd.own2 : nd.own;
+      for (int k = o.lo[0]; k < o.hi[0]; ++k)
+        for (int j = o.lo[1]; j < o.hi[1]; ++j)
+          for (int i = o.lo[2]; i < o.hi[2]; ++i) {
+            int64_t cell = (int64_t(k) * ny + j) * nx + i;
+            S.perm[next] = int32_t(cell);
+            S.iperm[cell] = int32_t(next);
+            ++next;
+          }
+    }
     S.n[s] = int32_t(next - S.first[s]);
     S.parent[s] = nd.parent;
     S.level[s] = nd.depth;
@@ -144,7 +165,9 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
     std::vector<int32_t>& u = U[s];
     for (int a = 0; a < 3; ++a)
       for (int side = 0; side < 2; ++side) {
+        if (a == 2 && nodes[s].ring) continue;  // a ring has no x-neighbours outside itself
         int plane = side == 0 ? b.lo[a] - 1 : b.hi[a];
+        if (a == 2 && px) plane = (plane + nx) % nx;
         if (plane < 0 || plane >= dims[a]) continue;
         Box f = b;
         f.lo[a] = plane;
@@ -256,6 +279,7 @@ std::string build_symbolic(int nz, int ny, int nx, const SymbolicOptions& opt, S
         int64_t cell = (int64_t(k) * ny + j) * nx + i;
         for (int d = 0; d < 7; ++d) {
           int kk = k + dk[d], jj = j + dj[d], ii = i + di[d];
+          if (px) ii = (ii + nx) % nx;
           if (kk < 0 || kk >= nz || jj < 0 || jj >= ny || ii < 0 || ii >= nx) continue;
           int64_t nb = (int64_t(kk) * ny + jj) * nx + ii;
           int32_t p = S.iperm[cell], q = S.iperm[nb];

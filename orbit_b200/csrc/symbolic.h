@@ -66,6 +66,7 @@ constexpr int kNumSched = 3;
 
 struct Symbolic {
   int nz = 0, ny = 0, nx = 0;
+  int periodic_x = 0;  // periodic longitude: columns i = 0 and i = nx - 1 are neighbours
   int64_t N = 0;
   int leaf_cells = 0;
   int nsuper = 0;
@@ -127,6 +128,7 @@ struct SymbolicOptions {
   int tc_min_n = 48;      // smallest pivot count of a tensor-core supernode (fp32 factors)
   int subtree_div = 0;    // > 0: whole-subtree solve tasks below fac_nnz / subtree_div; 0: none
   int fuse_max_n = kFrontMaxN;  // largest pivot count of a one-CTA front (0: none)
+  int periodic_x = 0;     // periodic longitude (needs nx >= 3)
 };
 
 // Build the symbolic analysis.  Returns an empty string on success, an

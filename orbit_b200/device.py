@@ -47,12 +47,24 @@ class MetDevice:
                 continue
             self.t[name] = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
         self.pressure_form = not bool(getattr(met, "concentration_state", True))
+        self.periodic = bool(getattr(met, "periodic_lon", False))
+        if self.periodic:
+            if self.nx < 3:
+                raise ValueError("a periodic-longitude grid needs nx >= 3")
+            for name in ("u_wrap", "u_plus_wrap", "u_minus_wrap", "kmu_wrap"):
+                a = getattr(met, name, None)
+                if a is None or (name == "kmu_wrap" and self.split):
+                    continue
+                self.t[name] = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64).reshape(self.nz, self.ny),
+                                               device=device)
         # state weights: rho in the concentration form, 1 in the pressure form
         rho = met.state_weights().reshape(-1)
         self.rho = torch.as_tensor(rho, device=device)
         self.struct = _lib.MetT(**{k: _lib.ptr(self.t.get(k)) for k in _MET_FIELDS},
                                 dlat=self.dlat, dlon=self.dlon, split=int(self.split),
-                                pressure_form=int(self.pressure_form))
+                                pressure_form=int(self.pressure_form), periodic_lon=int(self.periodic),
+                                **{k: _lib.ptr(self.t.get(k))
+                                   for k in ("u_wrap", "u_plus_wrap", "u_minus_wrap", "kmu_wrap")})
 
 
 def assemble_transport(met: MetDevice, with_rowsum: bool = False):
@@ -65,19 +77,34 @@ def assemble_transport(met: MetDevice, with_rowsum: bool = False):
     return (T, rs) if with_rowsum else T
 
 
-def stencil_to_csr(T: np.ndarray, nz: int, ny: int, nx: int):
-    """Host helper: scipy CSR of a [7, N] stencil (boundary entries dropped)."""
+def boundary_loss(met: MetDevice) -> torch.Tensor:
+    """Lateral boundary loss rate of every cell (N doubles, zero inside):
+    the open-outflow part of the transport block's diagonal at the x (not
+    on periodic grids) and y edges (operator.py:25-178)."""
+    out = torch.empty(met.N, dtype=torch.float64, device=met.rho.device)
+    _lib.check(_lib.lib().orbit_transport_boundary_loss(met.nz, met.ny, met.nx, C.byref(met.struct), _lib.ptr(out),
+                                                        _stream()))
+    return out
+
+
+def stencil_to_csr(T: np.ndarray, nz: int, ny: int, nx: int, periodic: bool = False):
+    """Host helper: scipy CSR of a [7, N] stencil (boundary entries dropped;
+    with ``periodic`` the W entry of column 0 and the E entry of column nx-1
+    are the wrap-face couplings to column nx-1 and column 0)."""
     import scipy.sparse as sp
     N = nz * ny * nx
     c = np.arange(N)
     k, r = np.divmod(c, nx * ny)
     j, i = np.divmod(r, nx)
-    off = [0, -1, 1, -nx, nx, -nx * ny, nx * ny]
-    ok = [np.ones(N, bool), i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1]
+    off = [np.zeros(N, np.int64), np.where(i > 0, -1, nx - 1), np.where(i < nx - 1, 1, -(nx - 1)),
+           -nx, nx, -nx * ny, nx * ny]
+    px = bool(periodic) and nx >= 3
+    ok = [np.ones(N, bool), (i > 0) | px, (i < nx - 1) | px, j > 0, j < ny - 1, k > 0, k < nz - 1]
     rows, cols, vals = [], [], []
     for d in range(7):
         m = ok[d]
-        rows.append(c[m]); cols.append(c[m] + off[d]); vals.append(T[d][m])
+        o = off[d][m] if isinstance(off[d], np.ndarray) else off[d]
+        rows.append(c[m]); cols.append(c[m] + o); vals.append(T[d][m])
     return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                          shape=(N, N))
 
@@ -135,13 +162,24 @@ def source_coupling(e: torch.Tensor, sources, out: Optional[torch.Tensor] = None
     return out
 
 
-def fct_source(met: MetDevice, c: torch.Tensor, dt: float = DTAU, limited: bool = True):
-    """K2: FCT deferred-correction source for one or more (N,) concentration vectors."""
+def fct_source(met: MetDevice, c: torch.Tensor, dt: float = DTAU, limited: bool = True,
+               c_ghost: Optional[torch.Tensor] = None):
+    """K2: FCT deferred-correction source for one or more (N,) concentration
+    vectors; ``c_ghost`` (same shape as ``c``) is the lateral-inflow field whose
+    edge-cell values stand for the cells beyond the lateral edges."""
     c2 = c.reshape(-1, met.N).contiguous()
     d = torch.empty_like(c2)
-    _lib.check(_lib.lib().orbit_fct_source(met.nz, met.ny, met.nx, C.byref(met.struct), c2.shape[0],
-                                           _lib.ptr(c2), float(dt), int(limited), _lib.ptr(d),
-                                           _stream()))
+    if c_ghost is None:
+        _lib.check(_lib.lib().orbit_fct_source(met.nz, met.ny, met.nx, C.byref(met.struct), c2.shape[0],
+                                               _lib.ptr(c2), float(dt), int(limited), _lib.ptr(d),
+                                               _stream()))
+    else:
+        g2 = c_ghost.reshape(-1, met.N).contiguous()
+        if g2.shape != c2.shape:
+            raise ValueError("c_ghost must have the shape of c")
+        _lib.check(_lib.lib().orbit_fct_source_ghost(met.nz, met.ny, met.nx, C.byref(met.struct), c2.shape[0],
+                                                     _lib.ptr(c2), _lib.ptr(g2), float(dt), int(limited),
+                                                     _lib.ptr(d), _stream()))
     return d.reshape(c.shape)
 
 
@@ -156,16 +194,19 @@ def fct_linear_operator(met: MetDevice, c_base: torch.Tensor, dt: float = DTAU) 
 
 
 def stencil_apply(nz: int, ny: int, nx: int, stencils: torch.Tensor, x: torch.Tensor, alpha: float = 1.0,
-                  trans: bool = False, out: Optional[torch.Tensor] = None, beta: float = 0.0) -> torch.Tensor:
-    """out = beta out + alpha S x (or S^T x) for [.., 7, N] stencils and [.., N] vectors."""
+                  trans: bool = False, out: Optional[torch.Tensor] = None, beta: float = 0.0,
+                  periodic: bool = False) -> torch.Tensor:
+    """out = beta out + alpha S x (or S^T x) for [.., 7, N] stencils and [.., N] vectors
+    (``periodic``: the W/E entries of columns 0 and nx-1 are the wrap couplings)."""
     N = nz * ny * nx
     S2 = stencils.reshape(-1, 7, N).contiguous()
     x2 = x.reshape(-1, N).contiguous()
     if S2.shape[0] != x2.shape[0]:
         raise ValueError("one stencil per vector")
     y = out if out is not None else torch.empty_like(x2)
-    _lib.check(_lib.lib().orbit_stencil_apply(nz, ny, nx, x2.shape[0], _lib.ptr(S2), _lib.ptr(x2), float(alpha),
-                                              float(beta), int(trans), _lib.ptr(y), _stream()))
+    _lib.check(_lib.lib().orbit_stencil_apply_grid(nz, ny, nx, int(bool(periodic)), x2.shape[0], _lib.ptr(S2),
+                                                   _lib.ptr(x2), float(alpha), float(beta), int(trans), _lib.ptr(y),
+                                                   _stream()))
     return y.reshape(x.shape)
 
 

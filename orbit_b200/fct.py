@@ -1,6 +1,6 @@
 """Drop-in for the reference's horizontal FCT correction (orbit/core/fct.py).
 
-``compute_horizontal_fct_source(grid, indexer, c_flat, dt)`` (fct.py:459-492)
+``compute_horizontal_fct_source(grid, indexer, c_flat, dt[, c_ghost_flat])`` (fct.py:459-492)
 runs the two-pass Zalesak-limited anti-diffusive source on the device (K2)
 and returns a host array like the reference.  ``fct_source_device`` keeps
 everything on the device for the deferred-correction loop.
@@ -23,13 +23,14 @@ def fct_source_device(met_device, c, dt=DTAU, limited=True):
 
 
 def compute_horizontal_fct_source(grid, indexer, c_flat, dt, limited=True, c_ghost_flat=None):
-    if c_ghost_flat is not None:
-        raise NotImplementedError("lateral-inflow ghost cells are not supported by the device path")
+    """``c_ghost_flat``: the lateral boundary inflow concentration, whose
+    edge-cell values stand for the cells beyond each lateral edge (fct.py:283-292)."""
     import torch
     from . import device
     md = device.MetDevice(met_from_griddata(grid))
     c = torch.as_tensor(np.asarray(c_flat, dtype=np.float64), device="cuda")
-    return device.fct_source(md, c, dt, limited).cpu().numpy()
+    gh = None if c_ghost_flat is None else torch.as_tensor(np.asarray(c_ghost_flat, dtype=np.float64), device="cuda")
+    return device.fct_source(md, c, dt, limited, c_ghost=gh).cpu().numpy()
 
 
 def fct_linear_operator_device(met_device, c_base, dt=DTAU):

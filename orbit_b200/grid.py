@@ -28,9 +28,9 @@ def _arr(g, name, default=None):
 
 
 def met_from_griddata(g) -> MetBin:
-    """MetBin view of a reference GridData (regional grids only)."""
-    if bool(getattr(g, "periodic_lon", False)):
-        raise NotImplementedError("periodic-longitude grids are not supported by the device path")
+    """MetBin view of a reference GridData (regional or periodic in longitude;
+    the wrap face reads UAvg_wrap, UAvg_plus/minus_wrap and K_meander_u_wrap,
+    grid_data.py:426-445)."""
     nz, ny, nx = int(g.nz), int(g.ny), int(g.nx)
     split = bool(getattr(g, "has_split_fluxes", False))
     u, v = _arr(g, "UAvg"), _arr(g, "VAvg")
@@ -73,7 +73,23 @@ def met_from_griddata(g) -> MetBin:
                   v_minus_n=np.maximum(-v_n, 0.0), kxxyy=_arr(g, "Kxxyy"), kzz=_arr(g, "Kzz"),
                   w_plus=w_plus, w_minus=w_minus, cmfmc=cm,
                   kmu=_arr(g, "K_meander_u", zeros), kmv=_arr(g, "K_meander_v", zeros), split=split,
-                  concentration_state=bool(getattr(g, "concentration_state", True)))
+                  concentration_state=bool(getattr(g, "concentration_state", True)), **_wrap_fields(g, nx, split))
+
+
+def _wrap_fields(g, nx, split):
+    if not (bool(getattr(g, "periodic_lon", False)) and nx > 1):
+        return {}
+    if nx < 3:
+        raise ValueError("a periodic-longitude grid needs nx >= 3 on the device path")
+    uw = _arr(g, "UAvg_wrap")
+    if uw is None:
+        raise ValueError("periodic-longitude grid without UAvg_wrap")
+    if split:
+        upw, umw = _arr(g, "UAvg_plus_wrap"), _arr(g, "UAvg_minus_wrap")
+    else:
+        upw, umw = np.maximum(uw, 0.0), np.maximum(-uw, 0.0)
+    return dict(periodic_lon=True, u_wrap=uw, u_plus_wrap=upw, u_minus_wrap=umw,
+                kmu_wrap=_arr(g, "K_meander_u_wrap", np.zeros_like(uw)))
 
 
 def griddata_like(m: MetBin, **extra) -> SimpleNamespace:
@@ -86,15 +102,19 @@ def griddata_like(m: MetBin, **extra) -> SimpleNamespace:
         U_minus_face_e=m.u_minus_e, V_face_n=m.v_n, V_plus_face_n=m.v_plus_n, V_minus_face_n=m.v_minus_n,
         Kzz=m.kzz, Kxxyy=m.kxxyy, K_meander_u=m.kmu, K_meander_v=m.kmv, omega_edge=w,
         omega_edge_plus=m.w_plus, omega_edge_minus=m.w_minus, has_interface_omega=True, CMFMC=m.cmfmc,
-        periodic_lon=False, concentration_state=bool(m.concentration_state))
+        periodic_lon=bool(m.periodic_lon), concentration_state=bool(m.concentration_state))
+    if m.periodic_lon:
+        ns.UAvg_wrap, ns.UAvg_plus_wrap, ns.UAvg_minus_wrap = m.u_wrap, m.u_plus_wrap, m.u_minus_wrap
+        ns.K_meander_u_wrap = m.kmu_wrap if m.kmu_wrap is not None else np.zeros_like(m.u_wrap)
     for k, v in extra.items():
         setattr(ns, k, v)
     return ns
 
 
-def stencil_from_matrix(M, nz: int, ny: int, nx: int) -> np.ndarray:
+def stencil_from_matrix(M, nz: int, ny: int, nx: int, periodic: bool = False) -> np.ndarray:
     """[7, N] stencil of a sparse matrix on the 7-point pattern (raises if an
-    entry lies outside it)."""
+    entry lies outside it).  With ``periodic`` the wrap-face couplings of
+    columns 0 and nx-1 go to their W and E entries."""
     import scipy.sparse as sp
     N = nz * ny * nx
     C = sp.csr_matrix(M)
@@ -115,6 +135,11 @@ def stencil_from_matrix(M, nz: int, ny: int, nx: int) -> np.ndarray:
             m &= ok
         st[d, rows[m]] = C.data[m]
         used |= m
+    if periodic and nx >= 3:
+        for d, o, ok in ((1, nx - 1, i == 0), (2, -(nx - 1), i == nx - 1)):
+            m = (off == o) & ok & ~used
+            st[d, rows[m]] += C.data[m]
+            used |= m
     if not np.all(used | (C.data == 0.0)):
         raise ValueError("matrix has entries outside the 7-point stencil of the grid")
     return st
@@ -122,14 +147,31 @@ def stencil_from_matrix(M, nz: int, ny: int, nx: int) -> np.ndarray:
 
 def infer_grid_shape(M):
     """(nz, ny, nx) of a 7-point operator from its off-diagonal offsets
-    (1, nx, nx*ny), or None when the pattern does not determine it."""
+    (1, nx, nx*ny, and nx-1 for the wrap face of a periodic-longitude grid),
+    or None when the pattern does not determine it."""
     import scipy.sparse as sp
     C = sp.csr_matrix(M)
     N = C.shape[0]
     rows = np.repeat(np.arange(N), np.diff(C.indptr))
     off = np.unique(np.abs(C.indices - rows))
     off = off[off > 0]
+    if len(off) == 4 and off[0] == 1 and off[1] + 1 == off[2]:
+        off = off[[0, 2, 3]]  # drop the wrap offset nx - 1
     if len(off) != 3 or off[0] != 1 or off[2] % off[1] or N % off[2]:
         return None
     nx, nxy = int(off[1]), int(off[2])
     return (N // nxy, nxy // nx, nx)
+
+
+def infer_periodic(M, shape) -> bool:
+    """True when the operator couples columns 0 and nx-1 of a row (the wrap
+    face of a periodic-longitude grid, convdiff.py:150-202)."""
+    import scipy.sparse as sp
+    nz, ny, nx = shape
+    if nx < 3:
+        return False
+    C = sp.csr_matrix(M)
+    rows = np.repeat(np.arange(C.shape[0]), np.diff(C.indptr))
+    off = C.indices - rows
+    i = rows % nx
+    return bool(np.any(((off == nx - 1) & (i == 0) | (off == -(nx - 1)) & (i == nx - 1)) & (C.data != 0.0)))

@@ -36,14 +36,24 @@ def transport_stencil(grid, with_rowsum=False):
     return device.assemble_transport(md, with_rowsum=with_rowsum)
 
 
+def _periodic(grid) -> bool:
+    return bool(getattr(grid, "periodic_lon", False)) and int(grid.nx) > 1
+
+
 def assemble_transport_block(grid, indexer=None, scheme: str = "exp", return_boundary_fluxes: bool = False):
+    """The transport block as a scipy CSC matrix (K1 on the device); with
+    ``return_boundary_fluxes`` also the lateral boundary loss rate of every
+    cell (compute_lateral_boundary_loss, operator.py:25-178), as the
+    reference returns them (operator.py:344-347)."""
     if scheme != "exp":
         raise ValueError(f"Only the Patankar exponential scheme is supported (got scheme={scheme!r})")
-    if return_boundary_fluxes:
-        raise NotImplementedError("return_boundary_fluxes is not provided by the device path")
-    from .device import stencil_to_csr
-    T = transport_stencil(grid).cpu().numpy()
-    return stencil_to_csr(T, int(grid.nz), int(grid.ny), int(grid.nx)).tocsc()
+    from . import device
+    md = device.MetDevice(met_from_griddata(grid))
+    T = device.assemble_transport(md).cpu().numpy()
+    Tc = device.stencil_to_csr(T, int(grid.nz), int(grid.ny), int(grid.nx), periodic=_periodic(grid)).tocsc()
+    if not return_boundary_fluxes:
+        return Tc
+    return Tc, device.boundary_loss(md).cpu().numpy()
 
 
 def species_operator(T, sink_diag):
@@ -165,7 +175,7 @@ def assemble_species_operators(grid, indexer=None, verbose: bool = True, scheme:
     d, k = device.species_diagonals(nz, ny, nx, f, a_photo, k_age, gain)
     d = d.cpu().numpy()
     k = k.cpu().numpy()
-    T = device.stencil_to_csr(Tst, nz, ny, nx).tocsc()
+    T = device.stencil_to_csr(Tst, nz, ny, nx, periodic=_periodic(grid)).tocsc()
     idx = np.arange(N)
 
     def diag(v):
@@ -182,7 +192,7 @@ def assemble_species_operators(grid, indexer=None, verbose: bool = True, scheme:
     for s in range(N_SPECIES):
         st = Tst.copy()
         st[0] = st[0] + d[s]
-        L_species.append(device.stencil_to_csr(st, nz, ny, nx).tocsc())
+        L_species.append(device.stencil_to_csr(st, nz, ny, nx, periodic=_periodic(grid)).tocsc())
     if verbose:
         print(f"{N_SPECIES} species operators on the device: {N:,} cells, couplings = {len(K_sources)}")
     if not return_D_per_species:

@@ -334,7 +334,7 @@ def _stencil(L, sym):
     from .grid import stencil_from_matrix
     if L is None:
         raise ValueError("operator already released (solved earlier in this call)")
-    return stencil_from_matrix(L, sym.nz, sym.ny, sym.nx)
+    return stencil_from_matrix(L, sym.nz, sym.ny, sym.nx, periodic=getattr(sym, "periodic", False))
 
 
 class _SlotView:

@@ -19,7 +19,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from .grid import infer_grid_shape, stencil_from_matrix
+from .grid import infer_grid_shape, infer_periodic, stencil_from_matrix
 from .symbolic import Symbolic
 from .synthetic import DTAU
 
@@ -52,12 +52,14 @@ def umfpack_symbolic(L, verbose: bool = True, ordering=None, qinit=None, grid_sh
     ``ordering`` and ``qinit`` are accepted for signature compatibility and
     ignored: the ordering is the geometric nested dissection of the grid.
     The grid shape comes from ``grid_shape``, else from the pattern of L
-    (off-diagonal offsets 1, nx, nx*ny), else from ``set_grid_shape``.
+    (off-diagonal offsets 1, nx, nx*ny), else from ``set_grid_shape``; a
+    periodic-longitude grid is recognised by L's wrap-face couplings between
+    columns 0 and nx-1.
     """
     shape = grid_shape or infer_grid_shape(L) or _default_shape
     if shape is None:
         raise ValueError("cannot determine the grid shape from L; pass grid_shape= or call set_grid_shape")
-    sym = Symbolic(*shape)
+    sym = Symbolic(*shape, periodic=infer_periodic(L, tuple(shape)))
     if sym.N != L.shape[0]:
         raise ValueError(f"grid {shape} has {sym.N} cells, L has {L.shape[0]} rows")
     if verbose:
@@ -96,7 +98,7 @@ class DeviceLU:
         self.sym = sym
         self.dtau = float(dtau)
         self.precision = int(precision)
-        self.stencil = stencil_from_matrix(L, sym.nz, sym.ny, sym.nx)
+        self.stencil = stencil_from_matrix(L, sym.nz, sym.ny, sym.nx, periodic=getattr(sym, "periodic", False))
         self.shape = (sym.N, sym.N)
         self.numeric_bytes = float(sym.info["factor_elems"] * (8 if precision == 64 else 4))
         self.peak_bytes = float(sym.info["front_elems"] * 2 * (8 if precision == 64 else 4))

@@ -25,14 +25,16 @@ INFO_KEYS = ("N", "nsuper", "nlevels", "factor_nnz", "factor_elems", "front_elem
 
 class Symbolic:
     def __init__(self, nz: int, ny: int, nx: int, leaf_cells: int = 0, chunk_elems: int = 0,
-                 tc_min_n: int = 0, subtree_div: int = -1):
+                 tc_min_n: int = 0, subtree_div: int = -1, periodic: bool = False):
         """Options left at 0 (subtree_div at -1) take the ORBIT_B200_* environment
         setting or the library default; `Symbolic.tuned` fills them from the
-        autotuner's cache."""
+        autotuner's cache.  ``periodic``: the grid wraps in longitude
+        (GridData.periodic_lon)."""
         L = _lib.lib()
         h = C.c_void_p()
-        _lib.check(L.orbit_symbolic_create_ex(int(nz), int(ny), int(nx), int(leaf_cells), int(chunk_elems),
-                                              int(tc_min_n), int(subtree_div), C.byref(h)))
+        _lib.check(L.orbit_symbolic_create_grid(int(nz), int(ny), int(nx), int(bool(periodic)), int(leaf_cells),
+                                                int(chunk_elems), int(tc_min_n), int(subtree_div), C.byref(h)))
+        self.periodic = bool(periodic)
         self.options = {"leaf_cells": int(leaf_cells), "chunk_elems": int(chunk_elems),
                         "tc_min_n": int(tc_min_n), "subtree_div": int(subtree_div)}
         self._h = h
@@ -66,11 +68,12 @@ class Symbolic:
         return out
 
     @classmethod
-    def tuned(cls, nz: int, ny: int, nx: int, precision: int = 32, batch: int = 12) -> "Symbolic":
+    def tuned(cls, nz: int, ny: int, nx: int, precision: int = 32, batch: int = 12,
+              periodic: bool = False) -> "Symbolic":
         """Analysis with the autotuner's cached options for this device, shape,
         precision and (nearest) batch width; the defaults if none are cached."""
         from .autotune import tuned_options
-        return cls(nz, ny, nx, **tuned_options((nz, ny, nx), precision, batch))
+        return cls(nz, ny, nx, periodic=periodic, **tuned_options((nz, ny, nx), precision, batch))
 
     def perm(self) -> np.ndarray:
         return self.array("perm")

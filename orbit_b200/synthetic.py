@@ -81,6 +81,13 @@ class MetBin:
     kmv: np.ndarray
     split: bool = True
     concentration_state: bool = True  # GridData.concentration_state (grid_data.py:71)
+    # periodic longitude (GridData.periodic_lon, grid_data.py:426-445): the
+    # wrap face between columns nx-1 and 0, (nz, ny) each
+    periodic_lon: bool = False
+    u_wrap: Optional[np.ndarray] = None
+    u_plus_wrap: Optional[np.ndarray] = None
+    u_minus_wrap: Optional[np.ndarray] = None
+    kmu_wrap: Optional[np.ndarray] = None
 
     @property
     def N(self) -> int:
@@ -176,8 +183,20 @@ def horizontal_row_sums(g: MetBin) -> np.ndarray:
         trl = np.where(ok, face / np.where(pl > 0, pl, 1.0), 1.0)
         r[:, :, 1:] += trr * (um - up) / d
         r[:, :, :-1] += trl * (up - um) / d
-    r[:, :, 0] += np.where(g.u_minus[:, :, 0] > 0, g.u_minus[:, :, 0], 0.0) / dx[:, :, 0]
-    r[:, :, -1] += np.where(g.u_plus_e > 0, g.u_plus_e, 0.0) / dx[:, :, -1]
+    if g.periodic_lon:
+        # wrap face: column nx-1 on its low side, column 0 on its high side
+        up, um = g.u_plus_wrap, g.u_minus_wrap
+        d = dx[:, :, 0]
+        pl, pr = dP[:, :, -1], dP[:, :, 0]
+        face = 0.5 * (pl + pr)
+        ok = (pl > 0) & (pr > 0)
+        trr = np.where(ok, face / np.where(pr > 0, pr, 1.0), 1.0)
+        trl = np.where(ok, face / np.where(pl > 0, pl, 1.0), 1.0)
+        r[:, :, 0] += trr * (um - up) / d
+        r[:, :, -1] += trl * (up - um) / d
+    else:
+        r[:, :, 0] += np.where(g.u_minus[:, :, 0] > 0, g.u_minus[:, :, 0], 0.0) / dx[:, :, 0]
+        r[:, :, -1] += np.where(g.u_plus_e > 0, g.u_plus_e, 0.0) / dx[:, :, -1]
     dy = g.dy
     dxc = g.dx
     if ny > 1:
@@ -202,8 +221,15 @@ def horizontal_row_sums(g: MetBin) -> np.ndarray:
 
 def make_met_bin(rng, nz, ny, nx, *, terrain_amp=0.0, rho_profile=False,
                  cmfmc_frac=0.0, lat0=5.0, lon0=60.0, dlat=0.5, dlon=0.625,
-                 wind_std=8.0, split=True) -> MetBin:
-    """Draw one bin of synthetic meteorology."""
+                 wind_std=8.0, split=True, periodic=False) -> MetBin:
+    """Draw one bin of synthetic meteorology.  With ``periodic`` the grid wraps
+    in longitude (dlon = 360 / nx) and the wrap face takes the mean of the
+    first and last staggered winds, as the reference's loader does
+    (grid_data.py:426-445)."""
+    if periodic:
+        if nx < 3:
+            raise ValueError("a periodic-longitude grid needs nx >= 3")
+        dlon = 360.0 / nx
     lat = lat0 + dlat * np.arange(ny)
     lon = lon0 + dlon * np.arange(nx)
     eta = np.linspace(0.0, 1.0, nz + 1)
@@ -246,6 +272,13 @@ def make_met_bin(rng, nz, ny, nx, *, terrain_amp=0.0, rho_profile=False,
                kxxyy=kxxyy, kzz=kzz,
                w_plus=np.zeros((nz + 1, ny, nx)), w_minus=np.zeros((nz + 1, ny, nx)),
                cmfmc=cmfmc, kmu=zeros3.copy(), kmv=zeros3.copy(), split=split)
+    if periodic:
+        uw = 0.5 * (U[:, :, 0] + U[:, :, nx])
+        g.periodic_lon = True
+        g.u_wrap = uw
+        g.u_plus_wrap = np.maximum(uw, 0.0)
+        g.u_minus_wrap = np.maximum(-uw, 0.0)
+        g.kmu_wrap = np.zeros((nz, ny))
     rh = horizontal_row_sums(g)
     w = np.zeros((nz + 1, ny, nx))
     w[1:] = np.cumsum(rh * dP, axis=0)

@@ -7,6 +7,7 @@ location is used unless ORBIT_REFERENCE is set):
     python tests/golden/make_golden.py --pressure-form   # only pressure_form.npz
     python tests/golden/make_golden.py --species         # only species_ops.npz
     python tests/golden/make_golden.py --closure         # only closure.npz
+    python tests/golden/make_golden.py --periodic        # only periodic.npz
 
 It builds reference ``GridData`` objects from this repository's seeded
 synthetic meteorology (``orbit_b200.synthetic``), calls the reference's own
@@ -57,7 +58,11 @@ def to_griddata(m: synthetic.MetBin, vd=None, wet=None) -> GridData:
     g.omega_edge, g.omega_edge_plus, g.omega_edge_minus = w, m.w_plus.copy(), m.w_minus.copy()
     g.has_interface_omega = True
     g.CMFMC = m.cmfmc.copy()
-    g.periodic_lon = False
+    g.periodic_lon = bool(m.periodic_lon)
+    if m.periodic_lon:
+        g.UAvg_wrap = m.u_wrap.copy()
+        g.UAvg_plus_wrap, g.UAvg_minus_wrap = m.u_plus_wrap.copy(), m.u_minus_wrap.copy()
+        g.K_meander_u_wrap = m.kmu_wrap.copy()
     z = np.zeros((m.nz, m.ny, m.nx))
     pdd = z.copy()
     if vd is not None:
@@ -76,6 +81,9 @@ def met_arrays(prefix, m):
                  "w_plus", "w_minus", "cmfmc", "kmu", "kmv", "lat", "lon"):
         out[f"{prefix}{name}"] = getattr(m, name)
     out[f"{prefix}meta"] = np.array([m.nz, m.ny, m.nx, m.dlat, m.dlon, float(m.split)])
+    if m.periodic_lon:
+        for name in ("u_wrap", "u_plus_wrap", "u_minus_wrap", "kmu_wrap"):
+            out[f"{prefix}{name}"] = getattr(m, name)
     return out
 
 
@@ -337,8 +345,78 @@ def closure():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def periodic():
+    """Goldens of periodic-longitude grids (GridData.periodic_lon): the
+    transport block with its wrap face (convdiff.py:150-202) in the split and
+    the non-split (meander) flux modes, the lateral boundary loss of
+    assemble_transport_block(..., return_boundary_fluxes=True) for a periodic
+    and a regional grid (operator.py:25-178, 344-347), the FCT source of a
+    periodic grid, the FCT source of regional grids with and without a
+    lateral-inflow (ghost) field, and one periodic orbit solved by the
+    reference's SuperLU path at tol 1e-12."""
+    rng = np.random.default_rng(31)
+    nz, ny, nx = 4, 6, 10
+    out = {}
+    for tag, split in (("ps_", True), ("pn_", False)):
+        m = synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=1500.0, rho_profile=True, cmfmc_frac=0.3,
+                                   wind_std=6.0, split=split, periodic=True)
+        if not split:
+            m.kmu = rng.uniform(0.0, 500.0, (nz, ny, nx))
+            m.kmu_wrap = rng.uniform(0.0, 500.0, (nz, ny))
+        idx = CellIndexer(nz, ny, nx)
+        g = to_griddata(m)
+        out.update(met_arrays(tag, m))
+        T, loss = operator.assemble_transport_block(g, idx, return_boundary_fluxes=True)
+        out.update(csc_arrays(f"{tag}T_", T))
+        out[f"{tag}loss"] = np.asarray(loss)
+        kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        c = ((1.0 + np.sin(0.7 * ii) * np.cos(0.5 * jj) + 0.2 * kk + rng.random((nz, ny, nx))) * 1e-9).reshape(-1)
+        out[f"{tag}c"] = c
+        out[f"{tag}fct_d"] = fct.compute_horizontal_fct_source(g, idx, c, DTAU)
+    # lateral loss of a regional grid (split and non-split)
+    for tag, split in (("rs_", True), ("rn_", False)):
+        m = synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=1500.0, rho_profile=True, wind_std=6.0,
+                                   split=split)
+        g = to_griddata(m)
+        out.update(met_arrays(tag, m))
+        idx = CellIndexer(nz, ny, nx)
+        _, loss = operator.assemble_transport_block(g, idx, return_boundary_fluxes=True)
+        out[f"{tag}loss"] = np.asarray(loss)
+        # FCT with a lateral-inflow field (fct.py:459-492 with c_ghost_flat)
+        kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        c = ((1.0 + np.cos(0.9 * ii) * np.sin(0.4 * jj) + 0.1 * kk + rng.random((nz, ny, nx))) * 1e-9).reshape(-1)
+        cg = (rng.uniform(0.2, 3.0, (nz, ny, nx)) * 1e-9).reshape(-1)
+        out[f"{tag}c"], out[f"{tag}cg"] = c, cg
+        out[f"{tag}fct_dg"] = fct.compute_horizontal_fct_source(g, idx, c, DTAU, c_ghost_flat=cg)
+        out[f"{tag}fct_dg_unlim"] = fct.compute_horizontal_fct_source(g, idx, c, DTAU, limited=False,
+                                                                      c_ghost_flat=cg)
+        out[f"{tag}fct_d"] = fct.compute_horizontal_fct_source(g, idx, c, DTAU)
+    # one periodic orbit (eight periodic bins, one species)
+    met = [synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=1500.0, rho_profile=True, cmfmc_frac=0.3,
+                                  wind_std=6.0, periodic=True) for _ in range(N_BINS)]
+    spc = synthetic.make_species(4111, nz, ny, nx)
+    d = spc.sink_diag(met)
+    idx = CellIndexer(nz, ny, nx)
+    N = nz * ny * nx
+    I_N = sp.identity(N, format="csc")
+    lus = []
+    for t, m in enumerate(met):
+        out.update(met_arrays(f"om{t}_", m))
+        T = operator.assemble_transport_block(to_griddata(m), idx)
+        L = (T + sp.diags(d[t])).tocsc()
+        lus.append(_factor_one_bin(L, I_N, None, None))
+    orbit, info = solve_orbit_one_species(lus, [spc.emis[t] for t in range(N_BINS)], DTAU, tol=1e-12, maxiter=200)
+    out["o_vd"], out["o_wet"], out["o_loss"], out["o_emis"] = spc.vd, spc.wet, spc.loss, spc.emis
+    out["o_orbit"] = np.stack(orbit)
+    path = os.path.join(HERE, "periodic.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes; gmres iters", info["gmres_iters"])
+
+
 if __name__ == "__main__":
-    if "--pressure-form" in sys.argv:
+    if "--periodic" in sys.argv:
+        periodic()
+    elif "--pressure-form" in sys.argv:
         pressure_form()
     elif "--species" in sys.argv:
         species_operators()
@@ -349,3 +427,4 @@ if __name__ == "__main__":
         pressure_form()
         species_operators()
         closure()
+        periodic()

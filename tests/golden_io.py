@@ -30,8 +30,20 @@ def load_pressure_form():
 def met_bin(z, prefix):
     nz, ny, nx, dlat, dlon, split = z[f"{prefix}meta"]
     kw = {n: np.array(z[f"{prefix}{n}"]) for n in _NAMES}
+    if f"{prefix}u_wrap" in z:
+        kw["periodic_lon"] = True
+        for n in ("u_wrap", "u_plus_wrap", "u_minus_wrap", "kmu_wrap"):
+            kw[n] = np.array(z[f"{prefix}{n}"])
     return synthetic.MetBin(nz=int(nz), ny=int(ny), nx=int(nx), dlat=float(dlat),
                             dlon=float(dlon), split=bool(split), **kw)
+
+
+PERIODIC = os.path.join(os.path.dirname(GOLDEN), "periodic.npz")
+
+
+def load_periodic():
+    """Goldens of periodic-longitude grids (tests/golden/make_golden.py --periodic)."""
+    return dict(np.load(PERIODIC))
 
 
 def met_list(z):

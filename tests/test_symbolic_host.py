@@ -255,3 +255,43 @@ def test_one_pass_lu_with_inverses():
         assert np.abs(L @ U - F).max() <= 1e-12 * np.abs(F).max()
         assert np.abs(X - np.linalg.inv(L)).max() <= 1e-12
         assert np.abs(Z.T - np.linalg.inv(U)).max() <= 1e-12 * np.abs(np.linalg.inv(U)).max()
+
+
+def _periodic_matrix(nz, ny, nx, seed=5):
+    rng = np.random.default_rng(seed)
+    g = synthetic.make_met_bin(rng, nz, ny, nx, terrain_amp=2000.0, rho_profile=True, cmfmc_frac=0.4,
+                               periodic=True)
+    T = assembly.transport_block(g)
+    d = rng.uniform(1e-6, 1e-4, nz * ny * nx)
+    return (sp.eye(nz * ny * nx) + 10800.0 * assembly.species_operator(T, d)).tocsr()
+
+
+@pytest.mark.parametrize("shape,leaf", [((3, 4, 5), 4), ((4, 6, 9), 8), ((3, 9, 4), 6), ((5, 7, 12), 16)])
+def test_periodic_ring_dissection_replays_sparse_solve(shape, leaf):
+    """A longitude ring is cut by two planes (its first and middle columns);
+    the x-neighbours of boxes at columns 0 and nx-1 wrap around.  The replayed
+    supernodal factorization and sweeps reproduce scipy's solves with the
+    wrap-face couplings in A."""
+    from orbit_b200.grid import infer_grid_shape, infer_periodic, stencil_from_matrix
+    A = _periodic_matrix(*shape)
+    assert infer_grid_shape(A) == shape and infer_periodic(A, shape)
+    st = stencil_from_matrix(A, *shape, periodic=True)
+    sym = Symbolic(*shape, leaf_cells=leaf, periodic=True)
+    n, m, first = sym.array("n"), sym.array("m"), sym.array("first")
+    uoff, uidx = sym.array("uoff"), sym.array("uidx")
+    assert sorted(sym.array("perm").tolist()) == list(range(sym.N))
+    for s in range(len(n)):
+        assert np.all(np.diff(uidx[uoff[s]:uoff[s + 1]]) > 0)
+        assert np.all(uidx[uoff[s]:uoff[s + 1]] >= first[s] + n[s])
+    a, fac = _replay(sym, st)
+    rng = np.random.default_rng(2)
+    b = rng.standard_normal(sym.N)
+    xr = spla.spsolve(A.tocsc(), b)
+    assert np.abs(_solve(a, fac, b, trans=False) - xr).max() <= 1e-11 * np.abs(xr).max()
+    xtr = spla.spsolve(A.T.tocsc(), b)
+    assert np.abs(_solve(a, fac, b, trans=True) - xtr).max() <= 1e-11 * np.abs(xtr).max()
+
+
+def test_periodic_needs_three_columns():
+    with pytest.raises(Exception):
+        Symbolic(3, 4, 2, periodic=True)
