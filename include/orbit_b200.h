@@ -188,6 +188,23 @@ typedef struct {
   double aging_gain;               /* mass gained by the next-lower bin per unit aged */
 } orbit_species_fields_t;
 
+/* Oxidant fields of one bin for the archive-driven NOx -> TotalNO3 rate
+ * (device pointers, (nz, ny, nx) doubles; NULL where marked optional).  Field
+ * meaning follows GridData (orbit/core/grid_data.py:140-206). */
+typedef struct {
+  const double* temperature;   /* Temperature, K */
+  const double* pressure;      /* Pressure, Pa (layer centre) */
+  const double* oh;            /* archive_OH, molec/cm3 */
+  const double* no;            /* archive_NO, ppbv; optional */
+  const double* no2;           /* archive_NO2, ppbv */
+  const double* no3rad;        /* archive_NO3rad, ppbv; optional (no night channel without it) */
+  const double* p_s;           /* pS, ug/m3 of S; optional */
+  const double* p_nh;          /* pNH, ug/m3 of N; optional */
+  const double* p_no;          /* pNO, ug/m3 of N; optional */
+  const double* dust_fine;     /* ug/m3; optional */
+  const double* sea_salt_fine; /* ug/m3; optional */
+} orbit_oxidant_fields_t;
+
 /* K1b: the 14 species' diagonal sink rates d_s (wet deposition + surface
  * dry-deposition velocity / Dz + SOA photolysis + first-order chemistry
  * losses) and the diagonals of the six source couplings K[(target, source)]
@@ -198,6 +215,17 @@ typedef struct {
  * (orbit/core/operator.py:371-595): assemble_deposition
  * (orbit/core/deposition.py:101-146, 263-360), the SO2 oxidation blocks
  * (orbit/core/chemistry.py:13-47) and the VBS aging blocks. */
+/* Per-cell first-order NOx -> TotalNO3 rate (device, N doubles, 1/s): the
+ * daytime OH + NO2 channel (JPL Troe rate times [OH] times the NO2 share of
+ * NOx) plus, unless disable_night, N2O5 hydrolysis on fine aerosol (N2O5 in
+ * thermal equilibrium with NO2 and the NO3 radical, uptake 0.02 on the
+ * surface of 0.15 um spheres of the fine-mode mass).  Replaces
+ * build_nox_to_no3_rate (orbit/core/nox_to_no3_rate.py:94-155, with
+ * oxidants.py:142-206), which assemble_species_operators calls when a grid
+ * carries archive OH and no rate is given (operator.py:474-476). */
+int orbit_nox_to_no3_rate(int64_t n_cells, const orbit_oxidant_fields_t* f, int disable_night, double* rate,
+                          orbit_stream_t stream);
+
 int orbit_species_diagonals(int nz, int ny, int nx, const orbit_species_fields_t* fields, double* d,
                             double* k_src, orbit_stream_t stream);
 

@@ -11,6 +11,9 @@ bin given as a namespace with the reference GridData field names:
   ``_get_o3_vd``                          orbit/core/deposition.py:171-260
 * the diagonal chemistry and aging blocks of
   ``assemble_species_operators``          orbit/core/operator.py:419-585
+* ``build_nox_to_no3_rate``               orbit/core/nox_to_no3_rate.py:94-155
+  with ``air_density``, ``k_OH_NO2``, ``Keq_N2O5``, ``mean_speed_N2O5``
+                                          orbit/core/oxidants.py:142-206
 """
 from __future__ import annotations
 
@@ -110,3 +113,39 @@ def diagonals(g, partitioning="marginal", a_photo=0.0, so2_ox=None, nox_ox=None,
             Kage[src] = r
             K[(dst, src)] = -aging_gain * r
     return d, K, D, Kage
+
+
+def nox_to_no3_rate(g, disable_night=False):
+    """NOx -> TotalNO3 first-order rate (1/s): OH + NO2 by day, N2O5
+    hydrolysis on fine aerosol by night; None without archive OH / NO2."""
+    oh, no2 = _f(g, "archive_OH"), _f(g, "archive_NO2")
+    if oh is None or no2 is None:
+        return None
+    NA, KB, R = 6.02214076e23, 1.380649e-23, 8.31446
+    T, P = _f(g, "Temperature"), _f(g, "Pressure")
+    M = P * NA / (R * T) * 1e-6
+    no = _f(g, "archive_NO")
+    no_m = no * 1e-9 * M if no is not None else np.zeros_like(oh)
+    no2_m = no2 * 1e-9 * M
+    nox = no_m + no2_m
+    safe = np.where(nox > 0, nox, 1.0)
+    f_no2 = np.where(nox > 0, no2_m / safe, 1.0)
+    k0 = 1.8e-30 * (T / 298.0) ** (-3.0) * M
+    ratio = k0 / 2.8e-11
+    k_oh = (k0 / (1.0 + ratio)) * 0.6 ** (1.0 / (1.0 + np.log10(ratio) ** 2))
+    k_day = k_oh * oh * f_no2
+    k_night = np.zeros_like(k_day)
+    no3 = _f(g, "archive_NO3rad")
+    if not disable_night and no3 is not None:
+        n2o5 = 5.8e-27 * np.exp(10840.0 / T) * no2_m * (no3 * 1e-9 * M)
+        fine = np.zeros_like(T)
+        for name, ratio_c in (("pS", 96.0632 / 32.0655), ("pNH", 18.03851 / 14.0067), ("pNO", 62.00501 / 14.0067),
+                              ("dust_fine", 1.0), ("sea_salt_fine", 1.0)):
+            a = _f(g, name)
+            if a is not None:
+                fine = fine + (a * ratio_c if ratio_c != 1.0 else a)
+        area = fine * 1e-9 * (3.0 / (1700.0 * 0.15e-6)) * 1e-2
+        v = np.sqrt(8.0 * KB * T / (np.pi * (108.01e-3 / NA))) * 100.0
+        k_het = 0.25 * 0.02 * v * area
+        k_night = np.where(nox > 0, 2.0 * k_het * n2o5 / safe, 0.0)
+    return k_day + k_night

@@ -48,6 +48,12 @@ class SpeciesFieldsT(C.Structure):
         ("k_age", C.c_double), ("aging_gain", C.c_double)]
 
 
+class OxidantFieldsT(C.Structure):
+    """orbit_oxidant_fields_t (include/orbit_b200.h)."""
+    _fields_ = [(n, C.c_void_p) for n in ("temperature", "pressure", "oh", "no", "no2", "no3rad", "p_s", "p_nh",
+                                          "p_no", "dust_fine", "sea_salt_fine")]
+
+
 class LutT(C.Structure):
     """orbit_lut_t (include/orbit_b200.h)."""
     _fields_ = [("axis", C.c_void_p * 7), ("n", C.c_int * 7), ("field", C.c_void_p * 4)]
@@ -74,6 +80,7 @@ EXPORTS = {
                                                 C.c_void_p]),
     "orbit_mass_balance_rows": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p]),
+    "orbit_nox_to_no3_rate": (C.c_int, [C.c_int64, C.POINTER(OxidantFieldsT), C.c_int, C.c_void_p, C.c_void_p]),
     "orbit_species_diagonals": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(SpeciesFieldsT), C.c_void_p,
                                           C.c_void_p, C.c_void_p]),
     "orbit_source_coupling": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -149,10 +149,70 @@ __global__ void k_source_coupling(int64_t N, int n_src, CouplingSrc S, const dou
   }
 }
 
+// Archive-driven NOx -> TotalNO3 rate, one thread per cell
+// (nox_to_no3_rate.py:94-155; oxidants.py:142-206 for the JPL rate, the N2O5
+// equilibrium constant, the air number density and the N2O5 mean speed).
+constexpr double kAvogadro = 6.02214076e23;
+constexpr double kBoltzmann = 1.380649e-23;
+constexpr double kRGas = 8.31446;
+constexpr double kPi = 3.14159265358979323846;
+// element-to-compound mass ratios (orbit/core/constants.py:9-15)
+constexpr double kSToSO4 = 96.0632 / 32.0655;
+constexpr double kNToNH4 = 18.03851 / 14.0067;
+constexpr double kNToNO3 = 62.00501 / 14.0067;
+
+__global__ void k_nox_rate(int64_t N, orbit_oxidant_fields_t f, int night, double* __restrict__ rate) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const double T = f.temperature[c], P = f.pressure[c];
+  const double M = P * kAvogadro / (kRGas * T) * 1e-6;  // molec/cm3
+  const double no = f.no ? f.no[c] * 1e-9 * M : 0.0;
+  const double no2 = f.no2[c] * 1e-9 * M;
+  const double nox = no + no2;
+  const double safe = nox > 0.0 ? nox : 1.0;
+  const double f_no2 = nox > 0.0 ? no2 / safe : 1.0;
+  // OH + NO2 (+M): JPL Troe form, k0 = 1.8e-30 (T/298)^-3 M, kinf = 2.8e-11, Fc = 0.6
+  const double k0 = 1.8e-30 * pow(T / 298.0, -3.0) * M;
+  const double ratio = k0 / 2.8e-11;
+  const double lg = log10(ratio);
+  const double k_oh = (k0 / (1.0 + ratio)) * pow(0.6, 1.0 / (1.0 + lg * lg));
+  const double k_day = k_oh * f.oh[c] * f_no2;
+  double k_night = 0.0;
+  if (night && f.no3rad) {
+    const double no3 = f.no3rad[c] * 1e-9 * M;
+    const double n2o5 = 5.8e-27 * exp(10840.0 / T) * no2 * no3;
+    double fine = 0.0;  // ug/m3 of compound mass
+    if (f.p_s) fine = fine + f.p_s[c] * kSToSO4;
+    if (f.p_nh) fine = fine + f.p_nh[c] * kNToNH4;
+    if (f.p_no) fine = fine + f.p_no[c] * kNToNO3;
+    if (f.dust_fine) fine = fine + f.dust_fine[c];
+    if (f.sea_salt_fine) fine = fine + f.sea_salt_fine[c];
+    const double area = fine * 1e-9 * (3.0 / (1700.0 * 0.15e-6)) * 1e-2;  // cm2/cm3
+    const double v = sqrt(8.0 * kBoltzmann * T / (kPi * (108.01e-3 / kAvogadro))) * 100.0;  // cm/s
+    const double k_het = 0.25 * 0.02 * v * area;
+    k_night = nox > 0.0 ? 2.0 * k_het * n2o5 / safe : 0.0;
+  }
+  rate[c] = k_day + k_night;
+}
+
 }  // namespace
 }  // namespace orbit
 
 extern "C" {
+
+int orbit_nox_to_no3_rate(int64_t n_cells, const orbit_oxidant_fields_t* f, int disable_night, double* rate,
+                          orbit_stream_t stream) {
+  using namespace orbit;
+  if (!f || !rate || n_cells < 1 || !f->temperature || !f->pressure || !f->oh || !f->no2) {
+    set_last_error("orbit_nox_to_no3_rate: missing argument or required field (T, P, OH, NO2)");
+    return ORBIT_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  k_nox_rate<<<(unsigned)((n_cells + 127) / 128), 128, 0, st>>>(n_cells, *f, disable_night ? 0 : 1, rate);
+  note_launch();
+  ORBIT_CUDA_TRY(cudaGetLastError());
+  return ORBIT_OK;
+}
 
 int orbit_species_diagonals(int nz, int ny, int nx, const orbit_species_fields_t* f, double* d, double* k_src,
                             orbit_stream_t stream) {

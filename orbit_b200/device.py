@@ -143,6 +143,30 @@ def species_diagonals(nz: int, ny: int, nx: int, fields: dict, a_photo: float = 
     return d, k
 
 
+OXIDANT_FIELD_NAMES = ("temperature", "pressure", "oh", "no", "no2", "no3rad", "p_s", "p_nh", "p_no", "dust_fine",
+                       "sea_salt_fine")
+
+
+def nox_to_no3_rate(fields: dict, disable_night: bool = False, device="cuda") -> torch.Tensor:
+    """Archive-driven NOx -> TotalNO3 rate (1/s) per cell from the oxidant
+    fields (names as ``OXIDANT_FIELD_NAMES``; optional ones may be missing or None)."""
+    _require_cuda()
+    t = {}
+    n = None
+    for name in OXIDANT_FIELD_NAMES:
+        a = fields.get(name)
+        if a is None:
+            continue
+        t[name] = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64).reshape(-1), device=device)
+        n = t[name].numel()
+    if n is None:
+        raise ValueError("no oxidant fields given")
+    st = _lib.OxidantFieldsT(**{k: _lib.ptr(v) for k, v in t.items()})
+    out = torch.empty(n, dtype=torch.float64, device=device)
+    _lib.check(_lib.lib().orbit_nox_to_no3_rate(n, C.byref(st), int(bool(disable_night)), _lib.ptr(out), _stream()))
+    return out
+
+
 def source_coupling(e: torch.Tensor, sources, out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """out[tau] = e[tau] - sum over sources of kdiag[tau] * c[tau + shift] for one
     target species; ``sources`` is a list of (kdiag (8, N), orbit (9, N), shift)."""

@@ -85,6 +85,22 @@ def _field(grid, name):
     return a if a.size else None
 
 
+def build_nox_to_no3_rate(grid, disable_night: bool = False):
+    """Drop-in for orbit/core/nox_to_no3_rate.py::build_nox_to_no3_rate
+    (94-155): the per-cell NOx -> TotalNO3 rate (1/s) from the grid's archive
+    oxidants, computed on the device (K1b); None when archive_OH or
+    archive_NO2 is empty, as the reference returns."""
+    from . import device
+    if _field(grid, "archive_OH") is None or _field(grid, "archive_NO2") is None:
+        return None
+    names = {"temperature": "Temperature", "pressure": "Pressure", "oh": "archive_OH", "no": "archive_NO",
+             "no2": "archive_NO2", "no3rad": "archive_NO3rad", "p_s": "pS", "p_nh": "pNH", "p_no": "pNO",
+             "dust_fine": "dust_fine", "sea_salt_fine": "sea_salt_fine"}
+    f = {k: _field(grid, v) for k, v in names.items()}
+    shape = (int(grid.nz), int(grid.ny), int(grid.nx))
+    return device.nox_to_no3_rate(f, disable_night).cpu().numpy().reshape(shape)
+
+
 def _partition_fields(grid, partitioning):
     """The TotalNH and TotalNO3 particle fractions the reference blends with
     (_nh_partitioning, _get_no3_partitioning: deposition.py:171-216)."""
@@ -129,8 +145,7 @@ def species_fields(grid, partitioning="marginal", so2_ox_rate=None, nox_to_no3_r
                        else _field(grid, "SO2oxidation"))
         oh = _field(grid, "archive_OH")
         if nox_to_no3_rate is None and oh is not None:
-            raise NotImplementedError("the archive-driven NOx -> TotalNO3 rate (build_nox_to_no3_rate) is not "
-                                      "computed by the device path; pass nox_to_no3_rate")
+            nox_to_no3_rate = build_nox_to_no3_rate(grid)  # operator.py:474-476
         for key, rate in (("nox_ox", nox_to_no3_rate), ("o3_loss", o3_loss_rate), ("co_loss", co_loss_rate)):
             f[key] = np.asarray(rate, dtype=np.float64).reshape(nz, ny, nx) if rate is not None else None
         if oh is not None:

@@ -8,6 +8,7 @@ location is used unless ORBIT_REFERENCE is set):
     python tests/golden/make_golden.py --species         # only species_ops.npz
     python tests/golden/make_golden.py --closure         # only closure.npz
     python tests/golden/make_golden.py --periodic        # only periodic.npz
+    python tests/golden/make_golden.py --nox             # only nox_rate.npz
 
 It builds reference ``GridData`` objects from this repository's seeded
 synthetic meteorology (``orbit_b200.synthetic``), calls the reference's own
@@ -413,8 +414,44 @@ def periodic():
     print("wrote", path, os.path.getsize(path), "bytes; gmres iters", info["gmres_iters"])
 
 
+def nox_rate():
+    """Goldens of build_nox_to_no3_rate (nox_to_no3_rate.py:94-155): every
+    oxidant and aerosol field present, day and night channels; without NO,
+    NO3 radical and the optional aerosol fields; with the night channel off."""
+    from types import SimpleNamespace
+    from orbit.core.nox_to_no3_rate import build_nox_to_no3_rate
+    rng = np.random.default_rng(41)
+    nz, ny, nx = 4, 5, 6
+    sh = (nz, ny, nx)
+    full = dict(Temperature=rng.uniform(220.0, 305.0, sh), Pressure=rng.uniform(2.0e4, 1.02e5, sh),
+                archive_OH=rng.uniform(1e4, 1e7, sh), archive_NO=rng.uniform(0.0, 5.0, sh),
+                archive_NO2=rng.uniform(0.0, 20.0, sh), archive_NO3rad=rng.uniform(0.0, 0.05, sh),
+                pS=rng.uniform(0.0, 3.0, sh), pNH=rng.uniform(0.0, 2.0, sh), pNO=rng.uniform(0.0, 2.0, sh),
+                dust_fine=rng.uniform(0.0, 10.0, sh), sea_salt_fine=rng.uniform(0.0, 5.0, sh))
+    full["archive_NO2"][0, 0, :3] = 0.0  # NOx = 0 cells
+    full["archive_NO"][0, 0, :3] = 0.0
+    empty = np.array([])
+    cases = {"full": dict(full),
+             "lean": dict(full, archive_NO=empty, archive_NO3rad=empty, pNO=empty, dust_fine=empty)}
+    out = {}
+    for k, v in full.items():
+        out[f"nx_{k}"] = v
+    for tag, fields in cases.items():
+        g = GridData()
+        g.nz, g.ny, g.nx = nz, ny, nx
+        for k, v in fields.items():
+            setattr(g, k, v)
+        out[f"nx_rate_{tag}"] = build_nox_to_no3_rate(g)
+        out[f"nx_rate_{tag}_day"] = build_nox_to_no3_rate(g, disable_night=True)
+    path = os.path.join(HERE, "nox_rate.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    if "--periodic" in sys.argv:
+    if "--nox" in sys.argv:
+        nox_rate()
+    elif "--periodic" in sys.argv:
         periodic()
     elif "--pressure-form" in sys.argv:
         pressure_form()
@@ -428,3 +465,4 @@ if __name__ == "__main__":
         species_operators()
         closure()
         periodic()
+        nox_rate()

@@ -93,3 +93,44 @@ def test_device_species_operators_match_reference(tag, part, monkeypatch):
     Tref = golden_io.csc(Z, f"{key}_T_")
     assert _close(T.toarray(), Tref.toarray(), 1e-12)
     assert _close(L[1].toarray(), golden_io.csc(Z, f"{key}_L1_").toarray(), 1e-12)
+
+
+NOX = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "nox_rate.npz")))
+
+
+def _nox_grid(tag):
+    from types import SimpleNamespace
+    g = SimpleNamespace(nz=4, ny=5, nx=6)
+    for k in ("Temperature", "Pressure", "archive_OH", "archive_NO", "archive_NO2", "archive_NO3rad", "pS", "pNH",
+              "pNO", "dust_fine", "sea_salt_fine"):
+        setattr(g, k, NOX[f"nx_{k}"])
+    if tag == "lean":
+        for k in ("archive_NO", "archive_NO3rad", "pNO", "dust_fine"):
+            setattr(g, k, np.array([]))
+    return g
+
+
+@pytest.mark.parametrize("tag", ["full", "lean"])
+def test_oracle_nox_rate_matches_reference(tag):
+    """build_nox_to_no3_rate (nox_to_no3_rate.py:94-155): day + night and day only."""
+    from oracle import species as osp
+    g = _nox_grid(tag)
+    ref = NOX[f"nx_rate_{tag}"]
+    assert np.abs(osp.nox_to_no3_rate(g) - ref).max() <= 1e-12 * np.abs(ref).max()
+    ref_d = NOX[f"nx_rate_{tag}_day"]
+    assert np.abs(osp.nox_to_no3_rate(g, disable_night=True) - ref_d).max() <= 1e-12 * np.abs(ref_d).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["full", "lean"])
+def test_device_nox_rate_matches_reference(tag):
+    """K1b NOx -> TotalNO3 rate through the build_nox_to_no3_rate drop-in."""
+    from orbit_b200 import operator as dop
+    g = _nox_grid(tag)
+    for night, key in ((False, f"nx_rate_{tag}"), (True, f"nx_rate_{tag}_day")):
+        got = dop.build_nox_to_no3_rate(g, disable_night=night)
+        ref = NOX[key]
+        assert got.shape == ref.shape
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    g.archive_OH = np.array([])
+    assert dop.build_nox_to_no3_rate(g) is None
