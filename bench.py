@@ -474,7 +474,8 @@ def main():
         t_mixed = a.elapsed_time(b)
         fct = {"passes": passes, "tol": TOL, "mixed_batched_orbits_per_s": 1e3 * N_SPECIES / t_mixed,
                "mixed_batched_ms": t_mixed,
-               "all_converged": bool(all(np.all(i[:, 4] > 0) for i in infs))}
+               "all_converged": bool(all(np.all(i[:, 4] > 0) for i in infs)),
+               "chains_per_pass_mixed": [float(np.median(i[:, 7])) for i in infs]}
         if not args.no_plain:
             sym64 = Symbolic.tuned(NZ, NY, NX, 64, 1)
             fbp = device.FactorBatch(sym64, 1, 64)
@@ -490,6 +491,7 @@ def main():
                 tp.append(a.elapsed_time(b))
             fbp.close()
             fct["plain_fp64_orbits_per_s"] = 1e3 * len(tp) / sum(tp)
+            fct["chains_per_pass_plain"] = [float(i[0, 7]) for i in infp]
             fct["mixed_vs_plain"] = fct["mixed_batched_orbits_per_s"] / fct["plain_fp64_orbits_per_s"]
 
     # ---- roofline of the chained-solve kernel (K4) ----
