@@ -552,6 +552,11 @@ def main():
         fb.close()
         torch.cuda.empty_cache()
         serving = serve_bench.run(requests=args.serve_requests, rate=200.0, budget_gb=150.0)
+        # the same mix at a rate one GPU sustains (about a quarter of its
+        # throughput), where the latencies are service times, not queueing
+        light = serve_bench.run(requests=max(8, args.serve_requests // 5), rate=5.0, budget_gb=150.0, seed=6)
+        serving["light_load"] = {"arrival_rate_per_s": 5.0, "requests": light["requests"], "value": light["value"],
+                                 "latency_ms": light["latency_ms"], "all_converged": light["all_converged"]}
 
     cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
