@@ -349,10 +349,23 @@ def main():
     solve_only = {"value": orbits / (ms_solve / 1e3), "unit": "orbits/s", "ms_per_batch": ms_solve / args.steps}
 
     # ---- timed: end to end from pinned host buffers ----
-    import copy
-    keys = list(met_dev[0][0].t.keys())
-    pinned = [[{k: torch.from_numpy(np.ascontiguousarray(getattr(g, k), dtype=np.float64)).pin_memory()
-                for k in keys} for g in met] for met in mets]
+    # one pinned host block and one device block per met draw, the device
+    # fields re-pointed into it, so that a step's met input is one copy
+    flat_pin, flat_dev = [], []
+    for d, met in enumerate(mets):
+        parts = [m.t[k].cpu().numpy().reshape(-1) for m in met_dev[d] for k in list(m.t.keys())]
+        hp = torch.from_numpy(np.concatenate(parts)).pin_memory()
+        dv = torch.empty_like(hp, device="cuda")
+        dv.copy_(hp)
+        off = 0
+        for m in met_dev[d]:
+            for k in list(m.t.keys()):
+                sz = m.t[k].numel()
+                m.t[k] = dv[off:off + sz].view(m.t[k].shape)
+                off += sz
+            m.rebind()
+        flat_pin.append(hp)
+        flat_dev.append(dv)
     sinks_p = [torch.from_numpy(np.stack(sinks_h[d])).pin_memory() for d in range(args.draws)]
     emis_p = torch.from_numpy(emis_h).pin_memory()
     # Inputs and results move on a copy stream, double-buffered, so that step
@@ -364,7 +377,7 @@ def main():
     out_p = [torch.empty((N_SPECIES, 9, sym.N), dtype=torch.float64).pin_memory() for _ in range(2)]
     dev_sinks = [torch.empty((N_SPECIES, 8, sym.N), dtype=torch.float64, device="cuda") for _ in range(2)]
     dev_E = [torch.empty_like(E) for _ in range(2)]
-    h2d = sum(t.numel() * 8 for b in pinned[0] for t in b.values()) + sinks_p[0].numel() * 8 + emis_p.numel() * 8
+    h2d = flat_pin[0].numel() * 8 + sinks_p[0].numel() * 8 + emis_p.numel() * 8
     d2h = out_p[0].numel() * 8
     # two created streams: work on the legacy default stream would wait for
     # the copy stream and serialise the pipeline
@@ -375,9 +388,7 @@ def main():
     def enqueue_inputs(k):
         d, j = k % args.draws, k % 2
         with torch.cuda.stream(copy_st):
-            for b, m in enumerate(met_dev[d]):
-                for key in keys:
-                    m.t[key].copy_(pinned[d][b][key], non_blocking=True)
+            flat_dev[d].copy_(flat_pin[d], non_blocking=True)
             dev_sinks[j].copy_(sinks_p[d], non_blocking=True)
             dev_E[j].copy_(emis_p, non_blocking=True)
             ev_in[j].record(copy_st)

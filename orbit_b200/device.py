@@ -60,6 +60,11 @@ class MetDevice:
         # state weights: rho in the concentration form, 1 in the pressure form
         rho = met.state_weights().reshape(-1)
         self.rho = torch.as_tensor(rho, device=device)
+        self.rebind()
+
+    def rebind(self):
+        """Rebuild the C struct from ``self.t`` (after its tensors were replaced,
+        e.g. by views into one contiguous buffer that a single copy fills)."""
         self.struct = _lib.MetT(**{k: _lib.ptr(self.t.get(k)) for k in _MET_FIELDS},
                                 dlat=self.dlat, dlon=self.dlon, split=int(self.split),
                                 pressure_form=int(self.pressure_form), periodic_lon=int(self.periodic),
