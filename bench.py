@@ -490,6 +490,7 @@ def main():
         shared = {"rhs": n_rhs, "tol": stol, "factor_ms": t_fac,
                   "forward_orbits_per_s": 1e3 * n_rhs / t_f, "adjoint_orbits_per_s": 1e3 * n_rhs / t_a,
                   "forward_ms": t_f, "adjoint_ms": t_a,
+                  "chains_forward": float(np.median(inf_f[:, 7])), "chains_adjoint": float(np.median(inf_a[:, 7])),
                   "all_converged": bool(np.all(inf_f[:, 4] > 0) and np.all(inf_a[:, 4] > 0))}
         del fbS
 

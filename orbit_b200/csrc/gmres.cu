@@ -881,15 +881,22 @@ int orbit_solve_impl(orbit_factor_s* f, int n, const double* e_or_R, double dtau
       k_block_resid_T<<<gb, kVT, 0, st>>>(Rs, rho7, c.vs, f->E, Lb, f->A_stencil, sy->d.perm, sy->d.iperm, sy->S.nz,
                                           sy->S.ny, sy->S.nx, sy->S.periodic_x, d_ids, f->set_of);
       note_launch();
-      // s_rho: transposed sweep from X[8] = rho_7 with the shifted forcing
-      ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
-      k_lincomb<<<gb, kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, rho7, c.vs, zero, nullptr, 0, d_ids, N);
-      note_launch();
-      rc = launch_chain(f, B, d_ids, 1, 0, 8, Rs, 1.0, st);
-      if (rc) return rc;
-      for (int o : oact) mv[o]++;
-      k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, f->X, 9 * N, zero, nullptr, 0, d_ids, N);
-      note_launch();
+      if (it == 0 && !warm) {
+        // from lam = 0 the residual is rho_tau = A_tau^T R_tau, and the sweep
+        // of it ends (slot 0) where the sweep of the receptors s ends: reuse s
+        k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, c.Sv, c.vs, zero, nullptr, 0, d_ids, N);
+        note_launch();
+      } else {
+        // s_rho: transposed sweep from X[8] = rho_7 with the shifted forcing
+        ORBIT_CUDA_TRY(cudaMemsetAsync(f->X, 0, sizeof(double) * 9 * N * f->n_orbits, st));
+        k_lincomb<<<gb, kVT, 0, st>>>(f->X + 8 * N, 9 * N, one, rho7, c.vs, zero, nullptr, 0, d_ids, N);
+        note_launch();
+        rc = launch_chain(f, B, d_ids, 1, 0, 8, Rs, 1.0, st);
+        if (rc) return rc;
+        for (int o : oact) mv[o]++;
+        k_lincomb<<<gb, kVT, 0, st>>>(c.Dv, c.vs, one, f->X, 9 * N, zero, nullptr, 0, d_ids, N);
+        note_launch();
+      }
       rc = sqnorm(c, c.Dv, c.vs, d_ids, B, S_TMP);
       if (rc) return rc;
       rc = fetch_scal(c);
