@@ -169,3 +169,27 @@ def test_fct_ghost_field_matches_reference():
         for q in range(2):
             ref = ofct.fct_source(m, cc[q].cpu().numpy(), 10800.0, c_ghost_flat=gg[q].cpu().numpy())
             assert _rel(dd[q], ref) < 1e-12
+
+
+def test_periodic_orbit_through_the_dropin_modules():
+    """The reference's call sequence on a periodic grid: umfpack_symbolic(L)
+    recognises the wrap couplings of the CSC operator, _factor_one_bin gives
+    the device LU objects, solve_orbit_one_species the orbit (reference golden
+    at 1e-9); the LU objects' transposed solves match SuperLU's."""
+    from orbit_b200 import orbit as dorb
+    from orbit_b200.solve import umfpack_symbolic
+    met = [golden_io.met_bin(Z, f"om{t}_") for t in range(8)]
+    spc = synthetic.SpeciesFields(vd=Z["o_vd"], wet=Z["o_wet"], loss=Z["o_loss"], emis=Z["o_emis"])
+    d = spc.sink_diag(met)
+    L = [assembly.species_operator(assembly.transport_block(g), d[t]).tocsc() for t, g in enumerate(met)]
+    sym = umfpack_symbolic(L[0], verbose=False)
+    assert sym.sym.periodic
+    N = met[0].N
+    I_N = sp.identity(N, format="csc")
+    lus = [dorb._factor_one_bin(L[t], I_N, sym, None) for t in range(8)]
+    orb, info = dorb.solve_orbit_one_species(lus, [spc.emis[t] for t in range(8)], tol=1e-12)
+    assert _rel(np.stack(orb), Z["o_orbit"]) < 1e-9
+    b = np.random.default_rng(9).standard_normal(N)
+    A = (I_N + 10800.0 * L[3]).tocsc()
+    ref = sp.linalg.splu(A)
+    assert _rel(lus[3].solve(b, trans="T"), ref.solve(b, trans="T")) < 1e-12
