@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
+#include <vector>
 
 #include "common.cuh"
 #include "handles.h"
@@ -83,6 +84,7 @@ struct ChainDev {
   long long spin_limit;
   int never_ready;  // self-test: the first task waits for a count nothing reaches
   int prefetch;     // L2 prefetch of each task's factor rows before its dependency wait
+  int stream_ef;    // factor rows read once per launch: evict-first loads
   int64_t prefetch_bytes;  // at most this many bytes of a task's rows are prefetched
   unsigned spin_ns;  // longest sleep between polls of a completion counter
   int ngroups;  // task groups (orbits or right-hand-side groups) split into ngroups ...
@@ -212,12 +214,43 @@ __device__ __forceinline__ double dot16(const double2& a, const double* v) {
 #endif
 template <typename T> struct Depth { static constexpr int value = sizeof(T) == 4 ? ORBIT_SOLVE_DEPTH_FP32 : ORBIT_SOLVE_DEPTH_FP64; };
 
+// Factor rows that a launch reads once (every solve slot has its own factor
+// set) are loaded under an L2 evict-first policy, so that they do not push out
+// the lines the tasks' prefetches brought in, nor the solution vectors; where
+// slots share a set the rows are reused from L2 and load under the normal
+// policy (the many-right-hand-side kernel keeps plain loads).  Measured on the
+// 80x72x15 grid (8 bins, CUDA events): the 12-orbit FP32 chain 6.44-6.50 ms
+// with evict-first against 6.58-6.62 without a hint, 6.54 with no L1
+// allocation (alone or with evict-first), 6.57 with evict-last prefetches;
+// the single-orbit FP64 chain unchanged (1.72 ms); evict-first in the 64-RHS
+// kernels, where the groups share one set: 24.6 vs 20.9 ms transposed and
+// 22.0 vs 20.7 ms forward.
+__device__ __forceinline__ uint64_t stream_policy(bool evict_first) {
+  uint64_t pol;
+  if (evict_first) asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  else asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+__device__ __forceinline__ float4 ld_stream(const float4* p, uint64_t pol) {
+  float4 x;
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w) : "l"(p), "l"(pol));
+  return x;
+}
+
+__device__ __forceinline__ double2 ld_stream(const double2* p, uint64_t pol) {
+  double2 x;
+  asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(x.x), "=d"(x.y) : "l"(p), "l"(pol));
+  return x;
+}
+
 // Per-lane partial of sum_{j0 <= j < j1} a[j] v[j] for a group of G lanes
 // (gl = lane within the group; a 16-byte aligned at j = 0, v in shared memory,
 // 16-byte aligned).  16-byte loads, up to U in flight per lane: the unrolled
 // loop issues its guarded loads before it uses any of them.
 template <typename T, int G = 32, int U = Depth<T>::value>
-__device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0, int j1, int gl) {
+__device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0, int j1, int gl, uint64_t pol) {
   using V = typename Vec16<T>::type;
   constexpr int W = Vec16<T>::w;
   T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
@@ -233,7 +266,7 @@ __device__ __forceinline__ T dot_seg(const T* __restrict__ a, const T* v, int j0
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       x[u] = V{};
-      if (u == 0 || k + u * G < nv1) x[u] = __ldg(a4 + k + u * G);
+      if (u == 0 || k + u * G < nv1) x[u] = ld_stream(a4 + k + u * G, pol);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -330,6 +363,7 @@ __device__ __forceinline__ void fwd_node(const ChainDev<T>& D, int o, int tau, i
   const int n = D.n[s], m = D.m[s], first = D.first[s];
   const int ldn = D.ldn[s], ldm = D.ldm[s];
   const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+  const uint64_t pol = stream_policy(D.stream_ef != 0);
   double* Yo = D.Y + (int64_t)o * N;
   double* Wo = D.W + (int64_t)o * D.w_size;
   const int bin_in = trans ? tau + 1 : tau;
@@ -370,7 +404,7 @@ __device__ __forceinline__ void fwd_node(const ChainDev<T>& D, int o, int tau, i
     // rows of [SQ; Pb]: row i < n uses the strict lower part (unit diagonal)
     const int64_t woff = D.woff[s];
     auto partial = [&](auto g, int i, int gl) {
-      return dot_seg<T, decltype(g)::value>(SQ + (int64_t)i * ldn, vec, 0, i < n ? i : n, gl);
+      return dot_seg<T, decltype(g)::value>(SQ + (int64_t)i * ldn, vec, 0, i < n ? i : n, gl, pol);
     };
     auto store = [&](int i, T acc) {
       if (i < n) Yo[first + i] = (double)(vec[i] + acc);
@@ -417,6 +451,7 @@ __device__ __forceinline__ void bwd_node(const ChainDev<T>& D, int o, int tau, i
   const int ldn = D.ldn[s], ldm = D.ldm[s];
   const int n0pad = (n + 3) & ~3;
   const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+  const uint64_t pol = stream_policy(D.stream_ef != 0);
   const double* Yo = D.Y + (int64_t)o * N;
   const int bin_out = trans ? tau : tau + 1;
   double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
@@ -429,8 +464,8 @@ __device__ __forceinline__ void bwd_node(const ChainDev<T>& D, int o, int tau, i
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
     auto partial = [&](auto g, int i, int gl) {
       constexpr int G = decltype(g)::value;
-      return dot_seg<T, G>(SQ + (int64_t)i * ldn, vec, i, n, gl) +
-             dot_seg<T, G>(Qr + (int64_t)i * ldm, vec + n0pad, 0, m, gl);
+      return dot_seg<T, G>(SQ + (int64_t)i * ldn, vec, i, n, gl, pol) +
+             dot_seg<T, G>(Qr + (int64_t)i * ldm, vec + n0pad, 0, m, gl, pol);
     };
     auto store = [&](int i, T acc) { Xout[first + i] = (double)acc; };
     const int G = group_lanes<T, Depth<T>::value>(n - r0 + m);
@@ -468,6 +503,7 @@ __device__ void fwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
   const int n = D.n[s], m = D.m[s], first = D.first[s];
   const int ldn = D.ldn[s], ldm = D.ldm[s];
   const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+  const uint64_t pol = stream_policy(D.stream_ef != 0);
   double* Yo = D.Y + (int64_t)o * N;
   double* Wo = D.W + (int64_t)o * D.w_size;
   const int bin_in = trans ? tau + 1 : tau;
@@ -508,7 +544,7 @@ __device__ void fwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
       }
     } else {
       auto partial = [&](auto g, int i, int gl) {
-        return dot_seg<T, decltype(g)::value>(SQ + (int64_t)i * ldn, v, 0, i < n ? i : n, gl);
+        return dot_seg<T, decltype(g)::value>(SQ + (int64_t)i * ldn, v, 0, i < n ? i : n, gl, pol);
       };
       auto store = [&](int i, T acc) {
         if (i < n) Yo[first + i] = (double)(v[i] + acc);
@@ -543,6 +579,7 @@ __device__ void bwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
   const int ldn = D.ldn[s], ldm = D.ldm[s];
   const int n0pad = (n + 3) & ~3;
   const T* SQ = D.factors + ((int64_t)D.set_of[o] * D.n_bins + tau) * D.fac_size + D.fac_off[s];
+  const uint64_t pol = stream_policy(D.stream_ef != 0);
   const double* Yo = D.Y + (int64_t)o * N;
   const int bin_out = trans ? tau : tau + 1;
   double* Xout = D.X + ((int64_t)o * 9 + bin_out) * N;
@@ -554,8 +591,8 @@ __device__ void bwd_node_warp(const ChainDev<T>& D, int o, int tau, int s, bool 
     const T* Qr = SQ + (int64_t)(n + m) * ldn;
     auto partial = [&](auto g, int i, int gl) {
       constexpr int G = decltype(g)::value;
-      return dot_seg<T, G>(SQ + (int64_t)i * ldn, v, i, n, gl) +
-             dot_seg<T, G>(Qr + (int64_t)i * ldm, v + n0pad, 0, m, gl);
+      return dot_seg<T, G>(SQ + (int64_t)i * ldn, v, i, n, gl, pol) +
+             dot_seg<T, G>(Qr + (int64_t)i * ldm, v + n0pad, 0, m, gl, pol);
     };
     auto store = [&](int i, T acc) { Xout[first + i] = (double)acc; };
     const int G = group_lanes<T>(n + m);
@@ -1003,16 +1040,17 @@ __global__ void k_add_forcing(double* X, const double* E, const int* orbit_ids, 
 }
 
 // Bytes of each task's factor rows prefetched into L2 before its dependency
-// wait at large batches: the first 32 KB (ORBIT_B200_PREFETCH_KB; 0 = the
+// wait at large batches: the first 48 KB (ORBIT_B200_PREFETCH_KB; 0 = the
 // whole task).  With every resident CTA prefetching whole backward tasks (up
 // to 64 KB at the large-batch schedule) the prefetched lines can outgrow L2
-// and be fetched twice; at 12 orbits the 12-orbit FP32 chain took 6.58 ms with
-// a 32 KB window, 6.66 with 16 KB and 6.76 with 8 KB, while at 1 and 4 orbits
-// whole tasks were fastest.
+// and be fetched twice; with the evict-first row loads the 12-orbit FP32
+// chain took 6.43 ms with a 48 KB window, 6.46 with 32 KB, 6.49 with 64 KB,
+// 6.50 with 24 KB, 6.57 with 16 KB and 6.67 with whole tasks, while at 1 and
+// 4 orbits whole tasks were fastest.
 int64_t prefetch_limit_bytes() {
   static const int64_t b = [] {
     const char* e = std::getenv("ORBIT_B200_PREFETCH_KB");
-    const long long kb = e ? std::atoll(e) : 32;
+    const long long kb = e ? std::atoll(e) : 48;
     return kb > 0 ? (int64_t)kb * 1024 : (int64_t)1 << 40;
   }();
   return b;
@@ -1089,6 +1127,16 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   // the window bounds the prefetch only where the prefetched lines of all
   // resident CTAs outgrow L2 (large batches); small batches prefetch whole tasks
   D.prefetch_bytes = Bt > 6 ? prefetch_limit_bytes() : ((int64_t)1 << 40);
+  // evict-first factor loads only where no two solve slots share a factor set
+  D.stream_ef = 1;
+  {
+    std::vector<char> seen((size_t)std::max(f->n_sets, 1), 0);
+    for (int o = 0; o < f->n_orbits && D.stream_ef; ++o) {
+      const int st_o = f->h_set_of[o];
+      if (st_o < 0 || st_o >= f->n_sets || seen[st_o]) D.stream_ef = 0;
+      else seen[st_o] = 1;
+    }
+  }
   D.spin_ns = chain_spin_ns();
   D.ngroups = std::max(1, std::min(Bt, chain_phase_sets()));
   D.goff = D.ngroups > 1 ? std::max(1, D.nphase / D.ngroups) : 0;
