@@ -1072,6 +1072,20 @@ int chain_phase_sets() {
 // Longest sleep between polls of a completion counter (ORBIT_B200_SPIN_NS,
 // default 256 ns: 2.65 vs 2.77 ms for a single-orbit FP64 chain against a
 // 1 us cap, no change at 12 orbits; 4 us was slower).
+// Phases between the starts of successive staggered sets (ORBIT_B200_CHAIN_GOFF;
+// unset or 0: the phases of one bin divided by the number of sets).  Any
+// offset keeps every dependency claimed before its dependant (dependencies stay
+// inside one orbit, hence inside one set); the last set starts at most one
+// bin's phases after the first, which bounds the claim-slot table.
+int chain_set_offset(int nphase, int nsets) {
+  static const int v = [] {
+    const char* e = std::getenv("ORBIT_B200_CHAIN_GOFF");
+    return e ? std::atoi(e) : 0;
+  }();
+  const int g = v > 0 ? v : nphase / std::max(1, nsets);
+  return std::max(1, std::min(g, nphase / std::max(1, nsets - 1)));
+}
+
 unsigned chain_spin_ns() {
   static const unsigned v = [] {
     const char* e = std::getenv("ORBIT_B200_SPIN_NS");
@@ -1139,7 +1153,7 @@ int launch_chain_t(orbit_factor_s* f, double* X, int B, const int* d_orbit_ids, 
   }
   D.spin_ns = chain_spin_ns();
   D.ngroups = std::max(1, std::min(Bt, chain_phase_sets()));
-  D.goff = D.ngroups > 1 ? std::max(1, D.nphase / D.ngroups) : 0;
+  D.goff = D.ngroups > 1 ? chain_set_offset(D.nphase, D.ngroups) : 0;
   if (D.total <= 0) return ORBIT_OK;
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->counters, 0, sizeof(int) * (size_t)f->n_orbits * 16 * S.nsuper, st));
   ORBIT_CUDA_TRY(cudaMemsetAsync(f->task_counter, 0, sizeof(int), st));
